@@ -1,0 +1,338 @@
+// Direction-optimising BFS (north_star (c)): push levels run the GAS engine
+// with the bfs Program (Algorithms/BFS/bfs.h:28-298) over a vertex queue; pull
+// levels run a bottom-up sweep in which every unvisited vertex scans its
+// in-edges for a parent in the frontier bitmap and stops at the first hit.
+// The switch follows Beamer's rule: push -> pull when the next frontier's
+// out-edges exceed (unvisited edges)/alpha, pull -> push when the frontier
+// shrinks below nodes/beta. Depths are unique, so every schedule gives the
+// same labels as the reference's CPUBFS (Algorithms/BFS/bfs.cu:57-111).
+#include <cuda_runtime.h>
+
+#include <algorithm>
+
+#include <vector>
+
+#include "algo_util.cuh"
+#include "gas/driver.cuh"
+#include "gas/engine.cuh"
+#include "gas/programs.cuh"
+
+namespace mg {
+
+using BfsP = programs::bfs;
+constexpr int kVTS = 4;  // frontier entries per thread in the scan
+constexpr int kVT = 8;   // items per thread in the expand (NV = 2048)
+
+// Bottom-up level: warp per 32-vertex bitmap word, lane per vertex.
+__global__ void __launch_bounds__(kNT) k_bfs_pull(GasArgs<BfsP> a) {
+  __shared__ unsigned long long s_cnt, s_edges;
+  Ctl *ctl = a.ctl;
+  if (!ctl->active || ctl->mode != MODE_BITMAP) return;
+  const uint32_t level = ctl->level;
+  const uint32_t *cur = cur_bm(a, level);
+  uint32_t *nxt = nxt_bm(a, level);
+  uint32_t *visited = a.vl.d_visited;
+  const int32_t V = a.g.V;
+  const uint32_t words = ((uint32_t)V + 31) / 32;
+  const int32_t *coff = a.g.csc_offsets, *crow = a.g.csc_rows, *ro = a.g.row_offsets;
+  const int lane = lane_id();
+  if (threadIdx.x == 0) {
+    s_cnt = 0;
+    s_edges = 0;
+  }
+  __syncthreads();
+  unsigned long long my_cnt = 0, my_edges = 0;
+  const uint32_t nwarps = gridDim.x * kNW;
+  for (uint32_t w = blockIdx.x * kNW + warp_id(); w < words; w += nwarps) {
+    const uint32_t vis = visited[w];
+    const int v = (int)(w * 32 + lane);
+    bool found = false;
+    if (v < V && !((vis >> lane) & 1u)) {
+      const int beg = coff[v], end = coff[v + 1];
+      for (int e = beg; e < end; ++e) {
+        const int u = crow[e];
+        if ((__ldg(&cur[u >> 5]) >> (u & 31)) & 1u) {
+          found = true;
+          break;
+        }
+      }
+    }
+    const uint32_t bal = __ballot_sync(0xffffffffu, found);
+    if (lane == 0) {
+      nxt[w] = bal;
+      if (bal) visited[w] = vis | bal;
+      my_cnt += __popc(bal);
+    }
+    if (found) {
+      a.vl.d_labels[v] = (int)level + 1;
+      my_edges += (unsigned long long)(ro[v + 1] - ro[v]);
+    }
+  }
+  my_edges = warp_sum(my_edges);
+  if (lane == 0) {
+    if (my_cnt) atomicAdd(&s_cnt, my_cnt);
+    if (my_edges) atomicAdd(&s_edges, my_edges);
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    if (s_cnt) atomicAdd((unsigned long long *)&ctl->acc[0], s_cnt);
+    if (s_edges) atomicAdd(&ctl->next_edges, s_edges);
+  }
+}
+
+// Pull -> push conversion at the start of a level: ordered compaction of the
+// frontier bitmap into the queue (decoupled look-back), and clearing of the
+// bitmap the coming push level will fill.
+__global__ void __launch_bounds__(kNT) k_bm_to_queue(GasArgs<BfsP> a) {
+  constexpr int WPT = 4;
+  constexpr uint32_t TW = kNT * WPT;
+  __shared__ uint32_t s_red[kNW + 1];
+  __shared__ uint32_t s_tile, s_prefix;
+  __shared__ int s_fail;
+  Ctl *ctl = a.ctl;
+  if (!ctl->active || !ctl->convert) return;
+  const uint32_t level = ctl->level, epoch = ctl->epoch + 2;
+  const unsigned long long spin_limit = ctl->spin_limit;
+  const uint32_t *src = cur_bm(a, level);
+  uint32_t *clr = nxt_bm(a, level);
+  int32_t *Q = cur_queue(a, level);
+  const uint32_t words = ((uint32_t)a.g.V + 31) / 32;
+  const uint32_t ntiles = (words + TW - 1) / TW;
+  if (threadIdx.x == 0) s_fail = 0;
+  for (;;) {
+    const uint32_t tile = next_tile(&ctl->tile_ctr[3], &s_tile);
+    if (tile >= ntiles || s_fail) break;
+    const uint32_t wb = tile * TW + threadIdx.x * WPT;
+    uint32_t wv[WPT], c = 0;
+#pragma unroll
+    for (int k = 0; k < WPT; ++k) {
+      wv[k] = (wb + k < words) ? src[wb + k] : 0u;
+      if (wb + k < words) clr[wb + k] = 0u;
+      c += __popc(wv[k]);
+    }
+    uint32_t tot;
+    const uint32_t ex = cta_exclusive_sum(c, s_red, &tot);
+    if (warp_id() == 0) {
+      bool failed = false;
+      const uint32_t pre = lookback(a.status, tile, tot, epoch, spin_limit, &failed);
+      if (lane_id() == 0) {
+        s_prefix = pre;
+        if (failed) {
+          s_fail = 1;
+          raise_error(ctl, MG_ERR_TIMEOUT);
+        } else if (tile == ntiles - 1) {
+          ctl->frontier_size = pre + tot;
+        }
+      }
+    }
+    __syncthreads();
+    if (s_fail) break;
+    uint32_t pos = s_prefix + ex;
+#pragma unroll
+    for (int k = 0; k < WPT; ++k) {
+      uint32_t x = wv[k];
+      while (x) {
+        const int b = __ffs(x) - 1;
+        x &= x - 1;
+        if (pos < (uint32_t)a.g.V) Q[pos] = (int32_t)((wb + k) * 32 + b);
+        ++pos;
+      }
+    }
+  }
+}
+
+__global__ void k_bfs_level_end(Ctl *ctl, int32_t V, int64_t E, cudaGraphConditionalHandle h, int use_handle) {
+  if (threadIdx.x != 0) return;
+  if (ctl->active) {
+    const uint32_t mode = ctl->mode;
+    uint32_t n_next;
+    if (mode == MODE_BITMAP) {
+      unsigned long long *cnt = (unsigned long long *)&ctl->acc[0];
+      n_next = (uint32_t)*cnt;
+      *cnt = 0;
+      ctl->pull_levels += 1;
+    } else {
+      n_next = ctl->next_size;
+      ctl->push_levels += 1;
+    }
+    const unsigned long long m_next = ctl->next_edges;
+    ctl->visited_edges += m_next;
+    ctl->visited_count += n_next;
+    uint32_t new_mode = mode;
+    if (ctl->dir_policy == MG_DIR_PUSH) {
+      new_mode = MODE_QUEUE;
+    } else if (ctl->dir_policy == MG_DIR_PULL) {
+      new_mode = MODE_BITMAP;
+    } else if (mode == MODE_QUEUE) {
+      const double unvisited_edges = (double)E - (double)ctl->visited_edges;
+      if ((double)m_next > unvisited_edges / (double)ctl->alpha) new_mode = MODE_BITMAP;
+    } else {
+      if ((double)n_next < (double)V / (double)ctl->beta && n_next < ctl->frontier_size) new_mode = MODE_QUEUE;
+    }
+    ctl->convert = (mode == MODE_BITMAP && new_mode == MODE_QUEUE) ? 1u : 0u;
+    ctl->mode = new_mode;
+    ctl->level += 1;
+    ctl->frontier_size = n_next;
+    ctl->next_size = 0;
+    ctl->edge_total = 0;
+    ctl->exp_tiles = 0;
+    ctl->next_edges = 0;
+    ctl->epoch += 4;
+    for (int i = 0; i < 4; ++i) ctl->tile_ctr[i] = 0;
+    ctl->active = (n_next > 0 && ctl->level < ctl->max_iter && ctl->error == 0) ? 1u : 0u;
+  }
+  if (use_handle) cudaGraphSetConditional(h, ctl->active);
+}
+
+__global__ void k_bfs_init(Ctl *ctl, const int32_t *srcs, int32_t nsrc, int32_t *labels, uint32_t *visited,
+                           uint32_t *bm0, const int32_t *ro, uint32_t dir_policy, float alpha, float beta) {
+  __shared__ unsigned long long s_edges;
+  if (threadIdx.x == 0) s_edges = 0;
+  __syncthreads();
+  for (int i = threadIdx.x; i < nsrc; i += blockDim.x) {
+    const int v = srcs[i];
+    labels[v] = 0;
+    atomicOr(&visited[v >> 5], 1u << (v & 31));
+    atomicOr(&bm0[v >> 5], 1u << (v & 31));
+    atomicAdd(&s_edges, (unsigned long long)(ro[v + 1] - ro[v]));
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    ctl->visited_edges = s_edges;
+    ctl->visited_count = (unsigned long long)nsrc;
+    ctl->dir_policy = dir_policy;
+    ctl->alpha = alpha;
+    ctl->beta = beta;
+    ctl->mode = (dir_policy == MG_DIR_PULL) ? MODE_BITMAP : MODE_QUEUE;
+    ctl->convert = 0;
+  }
+}
+
+// Shared by mg_bfs, mg_bfs_roots and mg_bfs_batch.
+int bfs_run(mg_graph *g, const std::vector<int32_t> &roots, int32_t *depths, mg_stats *stats, const mg_options *o) {
+  mg_options dflt;
+  if (!o) {
+    mg_options_init(&dflt);
+    o = &dflt;
+  }
+  if (o->direction == MG_DIR_PULL || o->direction == MG_DIR_AUTO) {
+    // Pull needs in-edges; they exist for every graph (CSC or the symmetric CSR).
+  } else if (o->direction != MG_DIR_PUSH) {
+    return set_error(MG_ERR_ARG, "unknown direction policy");
+  }
+  cudaStream_t s = run_stream(g, o);
+  int st = ensure_workspace(g);
+  if (st != MG_OK) return st;
+  if ((st = prepare_run(g, s)) != MG_OK) return st;
+  Workspace &w = g->ws;
+  GasArgs<BfsP> a;
+  a.g = g->csr;
+  a.vl.d_labels = w.vbuf[0];
+  a.vl.d_visited = w.visited;
+  a.vl.nodes = (int)g->nodes;
+  a.vl.edges = (int)g->edges;
+  a.el.nodes = (int)g->nodes;
+  a.el.edges = (int)g->edges;
+  a.queue0 = w.queue[0];
+  a.queue1 = w.queue[1];
+  a.scan = w.scan;
+  a.part = w.part;
+  a.status = w.status;
+  a.bm0 = w.bm[0];
+  a.bm1 = w.bm[1];
+  a.changed = w.changed;
+  a.gather_tmp = w.gather_tmp;
+  a.gather_res = w.gather_tmp;
+  a.ctl = w.ctl;
+  a.expand_in = 0;
+  a.gather_dir = NO_GATHER_EDGES;
+  const int V = (int)g->nodes;
+  const uint32_t nsrc = (uint32_t)roots.size();
+  // Every level of a traversal settles at least one vertex, so V + 2 levels bound
+  // the device loop even if a Program never empties its frontier.
+  const uint32_t max_iter = (uint32_t)std::min<int64_t>(o->iter_num > 0 ? o->iter_num : 0, g->nodes + 2);
+  cudaError_t e = cudaMemcpyAsync(w.queue[0], roots.data(), nsrc * 4, cudaMemcpyHostToDevice, s);
+  if (e == cudaSuccess) e = cudaMemsetAsync(w.visited, 0, w.words * 4, s);
+  if (e == cudaSuccess) e = cudaMemsetAsync(w.bm[0], 0, w.words * 4, s);
+  if (e == cudaSuccess) e = cudaMemsetAsync(w.bm[1], 0, w.words * 4, s);
+  if ((st = cuda_status(e, "bfs init")) != MG_OK) return st;
+  const int grid = persistent_grid(g, o, 4);
+  k_fill_i32<<<g->num_sms * 4, 256, 0, s>>>(w.vbuf[0], BfsP::INIT_VALUE, V);
+  k_ctl_init<<<1, 32, 0, s>>>(w.ctl, nsrc, max_iter, (unsigned long long)o->spin_limit, MODE_QUEUE);
+  k_bfs_init<<<1, 256, 0, s>>>(w.ctl, w.queue[0], (int32_t)nsrc, w.vbuf[0], w.visited, w.bm[0], g->csr.row_offsets,
+                               (uint32_t)o->direction, (float)o->alpha, (float)o->beta);
+  count_launch(3);
+  if ((st = launch_check("bfs init kernels")) != MG_OK) return st;
+  const int32_t Vv = g->csr.V;
+  const int64_t E = g->edges;
+  LevelBody body = [=](cudaStream_t ss, cudaGraphConditionalHandle h, int use_h) {
+    k_bm_to_queue<<<grid, kNT, 0, ss>>>(a);
+    k_frontier_scan<BfsP, kVTS, kVT><<<grid, kNT, 0, ss>>>(a);
+    k_expand<BfsP, kVT><<<grid, kNT, 0, ss>>>(a);
+    k_bfs_pull<<<grid, kNT, 0, ss>>>(a);
+    k_bfs_level_end<<<1, 32, 0, ss>>>(a.ctl, Vv, E, h, use_h);
+  };
+  LoopResult res;
+  st = run_level_loop(g, s, "bfs/" + std::to_string(grid), 5, body, o->use_cuda_graph != 0, &res);
+  if (st != MG_OK) return st;
+  finish_run(g, res.ctl.level);
+  if (res.ctl.error) return set_error(res.ctl.error, "bfs: device reported " + std::string(mg_status_string(res.ctl.error)));
+  if (stats) {
+    stats->iterations = (int32_t)res.ctl.level;
+    stats->push_iterations = (int32_t)res.ctl.push_levels;
+    stats->pull_iterations = (int32_t)res.ctl.pull_levels;
+    stats->converged = res.ctl.active ? 0 : 1;
+    stats->device_ms = res.ms;
+    stats->vertices_reached = (int64_t)res.ctl.visited_count;
+    stats->edges_traversed = 0;
+    if (want_stats(o)) {
+      int64_t r = 0, ed = 0;
+      if ((st = reach_stats(g, s, w.vbuf[0], -1, 1, 1, &r, &ed)) != MG_OK) return st;
+      stats->vertices_reached = r;
+      stats->edges_traversed = ed;
+    }
+  }
+  return copy_out(s, depths, w.vbuf[0], (size_t)V * 4, o->outputs_on_device != 0);
+}
+
+}  // namespace mg
+
+using namespace mg;
+
+extern "C" {
+
+int mg_bfs(mg_graph *g, int32_t src, int32_t *depths, mg_stats *stats, const mg_options *opts) {
+  clear_error();
+  if (!g) return set_error(MG_ERR_ARG, "graph is NULL");
+  std::vector<int32_t> roots;
+  int st = check_sources(g, &src, 1, &roots);
+  if (st != MG_OK) return st;
+  return bfs_run(g, roots, depths, stats, opts);
+}
+
+int mg_bfs_roots(mg_graph *g, const int32_t *srcs, int32_t nsrc, int32_t *depths, mg_stats *stats,
+                 const mg_options *opts) {
+  clear_error();
+  if (!g) return set_error(MG_ERR_ARG, "graph is NULL");
+  std::vector<int32_t> roots;
+  int st = check_sources(g, srcs, nsrc, &roots);
+  if (st != MG_OK) return st;
+  return bfs_run(g, roots, depths, stats, opts);
+}
+
+int mg_bfs_batch(mg_graph *g, const int32_t *srcs, int32_t *depths, mg_stats *stats, const mg_options *opts) {
+  clear_error();
+  if (!g) return set_error(MG_ERR_ARG, "graph is NULL");
+  if (g->graph_offsets.empty()) return set_error(MG_ERR_UNSUPPORTED, "graph was not created with mg_graph_create_batch");
+  if (!srcs) return set_error(MG_ERR_ARG, "srcs is NULL");
+  const int ng = (int)g->graph_offsets.size() - 1;
+  std::vector<int32_t> roots((size_t)ng);
+  for (int i = 0; i < ng; ++i) {
+    const int64_t n_i = g->graph_offsets[i + 1] - g->graph_offsets[i];
+    if (srcs[i] < 0 || srcs[i] >= n_i) return set_error(MG_ERR_ARG, "batch source out of range in graph " + std::to_string(i));
+    roots[i] = (int32_t)(g->graph_offsets[i] + srcs[i]);
+  }
+  return bfs_run(g, roots, depths, stats, opts);
+}
+
+}  // extern "C"

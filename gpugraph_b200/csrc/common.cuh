@@ -1,0 +1,200 @@
+// Device-side building blocks shared by every kernel of the library: the
+// per-run control block, acquire/release accessors, bounded spin waits, warp and
+// CTA scans, and the decoupled look-back used for order-preserving compaction.
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "../../include/mapgraph_b200.h"
+
+#define MG_DEVINL __device__ __forceinline__
+
+namespace mg {
+
+constexpr int kWarp = 32;
+constexpr int kNT = 256;  // threads per CTA of the level-loop kernels
+constexpr int kNW = kNT / kWarp;
+
+// Frontier representation of the current level.
+enum : uint32_t { MODE_QUEUE = 0, MODE_BITMAP = 1 };
+
+// Device control block of one traversal. Lives in device memory; every
+// level-loop kernel reads the fields it needs at entry, so the kernels can be
+// captured once in a CUDA graph and replayed without host round trips.
+struct Ctl {
+  uint32_t level;           // current GAS iteration
+  uint32_t frontier_size;   // |F| of the current level (queue mode)
+  uint32_t next_size;       // |F| produced by the current level
+  uint32_t edge_total;      // sum of expanded degrees of the current frontier
+  uint32_t exp_tiles;       // expand tiles of the current level
+  uint32_t tile_ctr[4];     // dynamic tile counters (scan, expand, pull, convert)
+  uint32_t done_ctas[4];    // CTA completion counters ("last CTA" finalisers)
+  uint32_t epoch;           // look-back epoch base; never reset between runs
+  uint32_t mode;            // MODE_QUEUE / MODE_BITMAP of the current level
+  uint32_t next_mode;       // decided at the end of a level
+  uint32_t active;          // 1 while the loop must continue
+  uint32_t max_iter;        // iteration cap
+  int32_t error;            // MG_OK or MG_ERR_TIMEOUT/MG_ERR_OVERFLOW
+  uint32_t push_levels;
+  uint32_t pull_levels;
+  uint32_t dir_policy;      // MG_DIR_* (BFS)
+  uint32_t convert;         // 1: rebuild the queue from the bitmap at level start
+  float alpha, beta;        // direction-switch factors (BFS)
+  unsigned long long next_edges;     // sum of degrees of the next frontier
+  unsigned long long visited_edges;  // sum of degrees of visited vertices (BFS)
+  unsigned long long visited_count;
+  unsigned long long spin_limit;
+  double residual;          // PageRank L1 residual of the last iteration
+  double dangling;          // PageRank dangling mass of the current ranks
+  double acc[4];            // FP64 reduction slots
+};
+
+MG_DEVINL uint32_t ld_acquire(const uint32_t *p) {
+  uint32_t v;
+  asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+  return v;
+}
+MG_DEVINL unsigned long long ld_acquire(const unsigned long long *p) {
+  unsigned long long v;
+  asm volatile("ld.acquire.gpu.global.u64 %0, [%1];" : "=l"(v) : "l"(p) : "memory");
+  return v;
+}
+MG_DEVINL void st_release(unsigned long long *p, unsigned long long v) {
+  asm volatile("st.release.gpu.global.u64 [%0], %1;" ::"l"(p), "l"(v) : "memory");
+}
+MG_DEVINL void st_release(uint32_t *p, uint32_t v) {
+  asm volatile("st.release.gpu.global.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
+}
+MG_DEVINL uint32_t ld_volatile(const uint32_t *p) { return *(volatile const uint32_t *)p; }
+
+MG_DEVINL uint32_t lanemask_lt() {
+  uint32_t m;
+  asm("mov.u32 %0, %%lanemask_lt;" : "=r"(m));
+  return m;
+}
+MG_DEVINL int lane_id() { return threadIdx.x & 31; }
+MG_DEVINL int warp_id() { return threadIdx.x >> 5; }
+
+template <typename T>
+MG_DEVINL T warp_inclusive_sum(T x) {
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    T y = __shfl_up_sync(0xffffffffu, x, o);
+    if (lane_id() >= o) x += y;
+  }
+  return x;
+}
+template <typename T>
+MG_DEVINL T warp_sum(T x) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) x += __shfl_xor_sync(0xffffffffu, x, o);
+  return x;
+}
+
+// Exclusive CTA-wide scan of one value per thread (blockDim.x == kNT).
+// Returns the exclusive prefix; *total receives the CTA sum. Uses smem[kNW+1].
+template <typename T>
+MG_DEVINL T cta_exclusive_sum(T x, T *smem, T *total) {
+  T inc = warp_inclusive_sum(x);
+  if (lane_id() == 31) smem[warp_id()] = inc;
+  __syncthreads();
+  if (warp_id() == 0) {
+    T w = lane_id() < kNW ? smem[lane_id()] : T(0);
+    T wi = warp_inclusive_sum(w);
+    if (lane_id() < kNW) smem[lane_id()] = wi - w;
+    if (lane_id() == kNW - 1) smem[kNW] = wi;
+  }
+  __syncthreads();
+  T r = smem[warp_id()] + inc - x;
+  *total = smem[kNW];
+  __syncthreads();
+  return r;
+}
+
+// Records a device-side failure without faulting: the first error wins.
+MG_DEVINL void raise_error(Ctl *ctl, int code) { atomicCAS(&ctl->error, 0, code); }
+
+// ---------------------------------------------------------------------------
+// Decoupled look-back (single-pass prefix over tiles processed in tile order).
+// Status word: [epoch:30][flag:2][value:32]; a word from another epoch reads as
+// "not yet published", so the status array is never cleared between launches.
+// Tiles are handed out by an atomic counter, so every predecessor of a tile is
+// already running or done: a wait only ends by publication or by the bounded
+// spin limit, after which the tile reports MG_ERR_TIMEOUT.
+enum : uint32_t { LB_AGG = 1, LB_INC = 2 };
+
+MG_DEVINL unsigned long long lb_pack(uint32_t epoch, uint32_t flag, uint32_t v) {
+  return ((unsigned long long)((epoch << 2) | flag) << 32) | v;
+}
+
+// Called by warp 0 of the tile. Publishes the tile aggregate and returns the
+// exclusive prefix of all earlier tiles (valid in every lane of warp 0). On a
+// timeout returns 0 and sets *failed.
+MG_DEVINL uint32_t lookback(unsigned long long *status, uint32_t tile, uint32_t agg, uint32_t epoch,
+                            unsigned long long spin_limit, bool *failed) {
+  const int lane = lane_id();
+  const uint32_t ep = epoch & 0x3fffffffu;
+  if (tile == 0) {
+    if (lane == 0) st_release(&status[0], lb_pack(ep, LB_INC, agg));
+    return 0;
+  }
+  if (lane == 0) st_release(&status[tile], lb_pack(ep, LB_AGG, agg));
+  uint32_t prefix = 0;
+  int64_t p = (int64_t)tile - 1;
+  unsigned long long spins = 0;
+  while (true) {
+    int64_t idx = p - lane;
+    uint32_t flag = LB_INC, val = 0;
+    if (idx >= 0) {
+      unsigned long long s = ld_acquire(&status[idx]);
+      uint32_t hi = (uint32_t)(s >> 32);
+      flag = ((hi >> 2) == ep) ? (hi & 3u) : 0u;
+      val = (uint32_t)s;
+    }
+    uint32_t not_ready = __ballot_sync(0xffffffffu, flag == 0);
+    uint32_t inc_mask = __ballot_sync(0xffffffffu, flag == LB_INC);
+    // Lanes up to (and including) the nearest inclusive predecessor must be ready.
+    uint32_t need = inc_mask ? ((inc_mask & (0u - inc_mask)) << 1) - 1u : 0xffffffffu;
+    if (not_ready & need) {
+      if (++spins >= spin_limit) {
+        *failed = true;
+        return 0;
+      }
+      if (spins > 64) __nanosleep(64);
+      continue;
+    }
+    uint32_t contrib = (need >> lane) & 1u ? val : 0u;
+    prefix += warp_sum(contrib);
+    if (inc_mask) break;
+    p -= 32;
+  }
+  if (lane == 0) st_release(&status[tile], lb_pack(ep, LB_INC, prefix + agg));
+  return prefix;
+}
+
+// Grabs the next tile index for the whole CTA (thread 0 increments, broadcast via smem).
+MG_DEVINL uint32_t next_tile(uint32_t *ctr, uint32_t *smem_slot) {
+  __syncthreads();
+  if (threadIdx.x == 0) *smem_slot = atomicAdd(ctr, 1u);
+  __syncthreads();
+  return *smem_slot;
+}
+
+// "Last CTA out" detection: returns true in exactly one CTA, after every other
+// CTA of the grid has passed this point (their prior writes are visible).
+MG_DEVINL bool last_cta_done(uint32_t *counter, uint32_t *smem_flag) {
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    __threadfence();
+    uint32_t prev = atomicAdd(counter, 1u);
+    *smem_flag = (prev == gridDim.x - 1) ? 1u : 0u;
+    if (*smem_flag) {
+      __threadfence();
+      *counter = 0;  // ready for the next launch
+    }
+  }
+  __syncthreads();
+  return *smem_flag != 0;
+}
+
+}  // namespace mg

@@ -1,0 +1,161 @@
+#include <cuda_runtime.h>
+
+#include <cstring>
+
+#include "../host_util.h"
+#include "driver.cuh"
+#include "engine.cuh"
+
+namespace mg {
+
+__global__ void k_level_end(Ctl *ctl, cudaGraphConditionalHandle h, int use_handle) {
+  if (threadIdx.x != 0) return;
+  if (ctl->active) {
+    ctl->level += 1;
+    ctl->push_levels += 1;
+    ctl->frontier_size = ctl->next_size;
+    ctl->next_size = 0;
+    ctl->edge_total = 0;
+    ctl->exp_tiles = 0;
+    ctl->next_edges = 0;
+    ctl->epoch += 4;
+    for (int i = 0; i < 4; ++i) ctl->tile_ctr[i] = 0;
+    ctl->active = (ctl->frontier_size > 0 && ctl->level < ctl->max_iter && ctl->error == 0) ? 1u : 0u;
+  }
+  if (use_handle) cudaGraphSetConditional(h, ctl->active);
+}
+
+__global__ void k_fill_i32(int32_t *p, int32_t v, int64_t n) {
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+    p[i] = v;
+}
+
+__global__ void k_sequence_i32(int32_t *p, int64_t n) {
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+    p[i] = (int32_t)i;
+}
+
+__global__ void k_ctl_init(Ctl *ctl, uint32_t frontier_size, uint32_t max_iter, unsigned long long spin_limit,
+                           uint32_t mode) {
+  if (threadIdx.x != 0) return;
+  // The epoch keeps growing across runs so stale look-back words never match;
+  // the host zeroes the status words and the control block before the 30-bit
+  // field could wrap (see prepare_run).
+  const uint32_t epoch = ctl->epoch + 4;
+  Ctl c;
+  memset(&c, 0, sizeof(c));
+  c.epoch = epoch;
+  c.frontier_size = frontier_size;
+  c.max_iter = max_iter;
+  c.spin_limit = spin_limit;
+  c.mode = mode;
+  c.next_mode = mode;
+  c.active = (frontier_size > 0 && max_iter > 0) ? 1u : 0u;
+  *ctl = c;
+}
+
+int read_ctl(mg_graph *g, cudaStream_t s, Ctl *out) {
+  cudaError_t e = cudaMemcpyAsync(g->host_ctl, g->ws.ctl, sizeof(Ctl), cudaMemcpyDeviceToHost, s);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+  if (e == cudaSuccess) memcpy(out, g->host_ctl, sizeof(Ctl));
+  return cuda_status(e, "control block read");
+}
+
+int prepare_run(mg_graph *g, cudaStream_t s) {
+  if (g->epochs_used < (1ull << 27)) return MG_OK;
+  cudaError_t e = cudaMemsetAsync(g->ws.status, 0, g->ws.status_cap * 8, s);
+  if (e == cudaSuccess) e = cudaMemsetAsync(g->ws.ctl, 0, sizeof(Ctl), s);
+  g->epochs_used = 0;
+  return cuda_status(e, "status reset");
+}
+
+void finish_run(mg_graph *g, uint32_t levels) { g->epochs_used += 4ull * ((uint64_t)levels + 2); }
+
+static int build_graph(mg_graph *g, cudaStream_t s, const LevelBody &body, LoopCache *lc) {
+  cudaGraph_t graph = nullptr;
+  cudaGraphExec_t exec = nullptr;
+  cudaError_t e = cudaGraphCreate(&graph, 0);
+  cudaGraphConditionalHandle h = 0;
+  if (e == cudaSuccess) e = cudaGraphConditionalHandleCreate(&h, graph, 1, cudaGraphCondAssignDefault);
+  cudaGraphNode_t cnode;
+  alignas(cudaGraphNodeParams) unsigned char raw[sizeof(cudaGraphNodeParams)];
+  memset(raw, 0, sizeof(raw));
+  cudaGraphNodeParams &params = *reinterpret_cast<cudaGraphNodeParams *>(raw);
+  params.type = cudaGraphNodeTypeConditional;
+  params.conditional.handle = h;
+  params.conditional.type = cudaGraphCondTypeWhile;
+  params.conditional.size = 1;
+  if (e == cudaSuccess) e = cudaGraphAddNode(&cnode, graph, nullptr, 0, &params);
+  if (e == cudaSuccess) {
+    cudaGraph_t bodyg = params.conditional.phGraph_out[0];
+    e = cudaStreamBeginCaptureToGraph(s, bodyg, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal);
+    if (e == cudaSuccess) {
+      body(s, h, 1);
+      cudaGraph_t captured = nullptr;
+      cudaError_t e2 = cudaStreamEndCapture(s, &captured);
+      e = (e2 != cudaSuccess) ? e2 : cudaGetLastError();
+    }
+  }
+  if (e == cudaSuccess) e = cudaGraphInstantiate(&exec, graph, 0);
+  if (e != cudaSuccess) {
+    cudaGetLastError();
+    if (exec) cudaGraphExecDestroy(exec);
+    if (graph) cudaGraphDestroy(graph);
+    return cuda_status(e, "level-loop graph capture");
+  }
+  lc->graph = graph;
+  lc->exec = exec;
+  (void)g;
+  return MG_OK;
+}
+
+int run_level_loop(mg_graph *g, cudaStream_t s, const std::string &key, int kernels_per_level, const LevelBody &body,
+                   bool use_graph, LoopResult *res) {
+  cudaError_t e = cudaEventRecord(g->ev0, s);
+  if (e != cudaSuccess) return cuda_status(e, "event record");
+  bool graphed = false;
+  if (use_graph) {
+    auto it = g->loops.find(key);
+    if (it == g->loops.end()) {
+      LoopCache lc;
+      lc.kernels_per_level = kernels_per_level;
+      if (build_graph(g, s, body, &lc) == MG_OK) {
+        it = g->loops.emplace(key, lc).first;
+      } else {
+        clear_error();  // fall back to host-driven launches of the same kernels
+      }
+    }
+    if (it != g->loops.end()) {
+      e = cudaGraphLaunch(it->second.exec, s);
+      if (e != cudaSuccess) return cuda_status(e, "graph launch");
+      graphed = true;
+    }
+  }
+  if (!graphed) {
+    // Host-driven loop: a few levels per control-block check; levels after the
+    // end are no-ops because every kernel returns when ctl->active == 0.
+    for (;;) {
+      for (int k = 0; k < 4; ++k) {
+        body(s, 0, 0);
+        count_launch(kernels_per_level);
+      }
+      int st = launch_check("level kernels");
+      if (st != MG_OK) return st;
+      Ctl c;
+      if ((st = read_ctl(g, s, &c)) != MG_OK) return st;
+      if (!c.active) break;
+    }
+  }
+  e = cudaEventRecord(g->ev1, s);
+  if (e != cudaSuccess) return cuda_status(e, "event record");
+  int st = read_ctl(g, s, &res->ctl);
+  if (st != MG_OK) return st;
+  float ms = 0.f;
+  cudaEventElapsedTime(&ms, g->ev0, g->ev1);
+  res->ms = ms;
+  res->used_graph = graphed;
+  if (graphed) count_launch((int64_t)kernels_per_level * ((int64_t)res->ctl.level + 1));
+  return MG_OK;
+}
+
+}  // namespace mg

@@ -1,0 +1,438 @@
+// Generic Gather-Apply-Scatter engine for sm_100a, templated on a Program
+// functor struct with the reference's contract (Algorithms/SSSP/sssp.h:34-393):
+// typedefs DataType/MiscType/GatherType/VertexId/SizeT, INIT_VALUE,
+// allow_duplicates, policy selectors srcVertex/gatherOverEdges/applyOverEdges/
+// postApplyOverEdges/expandOverEdges (GASengine/Enums.h:2-25) and the device
+// functors gather_edge, gather_sum, apply, post_apply, expand_vertex,
+// expand_edge, contract with their upstream MapGraph signatures.
+//
+// One GAS iteration (reference loop: enactor_vertex_centric.cuh:3386-3630) is
+//   [gather] -> [apply] -> [post_apply] -> frontier scan -> expand+contract -> level end
+// Every kernel is persistent (grid = SMs x CTAs/SM), reads the frontier size
+// and level from the device control block, and never returns to the host, so
+// the whole level loop is captured once in a CUDA graph (WHILE conditional node
+// driven by the level-end kernel) instead of the reference's per-level
+// cudaDeviceSynchronize + D->H size copy (enactor_vertex_centric.cuh:3801-3845).
+//
+// Expand (replaces expand_atomic::Kernel, expand_atomic/cta.cuh:633-755, and the
+// two-phase kernel_scatter_mgpu, mgpukernel/kernel.cuh:63-180): the frontier scan
+// computes the exclusive degree prefix of the frontier with a decoupled
+// look-back and writes merge-path tile partitions over the item space
+// (one item per frontier vertex + one per edge). Each expand tile then holds
+// exactly NV items, whatever the degrees: a hub's adjacency is split over many
+// CTAs (grid-cooperative), a mid-degree list is swept by consecutive lanes of
+// one warp or CTA (warp/CTA-cooperative), and low-degree lists are packed
+// together, with consecutive lanes reading consecutive column indices.
+//
+// Contract (replaces contract_atomic::Kernel, contract_atomic/cta.cuh:529-629):
+// the Program's contract functor runs inline on every emitted edge, then a
+// next-frontier bitmap test-and-set removes duplicates exactly, and survivors
+// are compacted with warp ballots, a CTA scan and a decoupled look-back over
+// tiles, so the next frontier keeps a deterministic order and needs no global
+// atomics per element.
+#pragma once
+#include <cuda_runtime.h>
+
+#include <type_traits>
+
+#include "../common.cuh"
+#include "../graph.cuh"
+#include "enums.h"
+
+namespace mg {
+
+// Optional Program traits (detected; the reference programs need none).
+template <class P, class = void>
+struct skip_unchanged_trait : std::false_type {};
+template <class P>
+struct skip_unchanged_trait<P, std::void_t<decltype(P::skip_unchanged_vertices)>>
+    : std::integral_constant<bool, P::skip_unchanged_vertices> {};
+
+template <class P, class = void>
+struct track_next_edges_trait : std::false_type {};
+template <class P>
+struct track_next_edges_trait<P, std::void_t<decltype(P::track_next_edges)>>
+    : std::integral_constant<bool, P::track_next_edges> {};
+
+template <class P>
+struct GasArgs {
+  DevCsr g;
+  typename P::VertexType vl;
+  typename P::EdgeType el;
+  int32_t *queue0, *queue1;
+  uint32_t *scan;
+  int32_t *part;
+  unsigned long long *status;
+  uint32_t *bm0, *bm1;
+  uint8_t *changed;
+  typename P::GatherType *gather_tmp;  // contract scratch / apply input
+  typename P::GatherType *gather_res;  // gather phase output
+  Ctl *ctl;
+  int32_t expand_in;  // 1: expand over the transpose (EXPAND_IN_EDGES)
+  int32_t gather_dir; // GatherEdges value
+};
+
+template <class P>
+MG_DEVINL int32_t *cur_queue(const GasArgs<P> &a, uint32_t level) { return (level & 1) ? a.queue1 : a.queue0; }
+template <class P>
+MG_DEVINL int32_t *nxt_queue(const GasArgs<P> &a, uint32_t level) { return (level & 1) ? a.queue0 : a.queue1; }
+template <class P>
+MG_DEVINL uint32_t *cur_bm(const GasArgs<P> &a, uint32_t level) { return (level & 1) ? a.bm1 : a.bm0; }
+template <class P>
+MG_DEVINL uint32_t *nxt_bm(const GasArgs<P> &a, uint32_t level) { return (level & 1) ? a.bm0 : a.bm1; }
+
+// ---------------------------------------------------------------- gather ----
+// Warp per frontier vertex; lanes sweep the adjacency with stride 32 and the
+// partial results are combined with the Program's gather_sum in a fixed
+// butterfly order (deterministic). Replaces gather_mgpu (enactor:2104-2725).
+template <class P>
+__global__ void __launch_bounds__(kNT) k_gather(GasArgs<P> a) {
+  Ctl *ctl = a.ctl;
+  if (!ctl->active || ctl->mode != MODE_QUEUE) return;
+  const uint32_t level = ctl->level, n = ctl->frontier_size;
+  const int32_t *F = cur_queue(a, level);
+  typename P::gather_edge gedge;
+  typename P::gather_sum gsum;
+  typedef typename P::GatherType G;
+  const int lane = lane_id();
+  const uint32_t wstride = gridDim.x * kNW;
+  for (uint32_t i = blockIdx.x * kNW + warp_id(); i < n; i += wstride) {
+    const int v = F[i];
+    G acc = G();
+    bool has = false;
+    for (int pass = 0; pass < 2; ++pass) {
+      const bool in = (pass == 0);
+      if (in && !(a.gather_dir == GATHER_IN_EDGES || a.gather_dir == GATHER_ALL_EDGES)) continue;
+      if (!in && !(a.gather_dir == GATHER_OUT_EDGES || a.gather_dir == GATHER_ALL_EDGES)) continue;
+      const int32_t *off = in ? a.g.csc_offsets : a.g.row_offsets;
+      const int32_t *nb = in ? a.g.csc_rows : a.g.col;
+      const int beg = off[v], end = off[v + 1];
+      for (int e = beg + lane; e < end; e += 32) {
+        const int u = nb[e];
+        const int eid = (in && a.g.csc_eid) ? a.g.csc_eid[e] : e;
+        G val;
+        gedge(v, eid, u, a.vl, a.el, val);
+        acc = has ? gsum(acc, val) : val;
+        has = true;
+      }
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+      G oacc = __shfl_xor_sync(0xffffffffu, acc, o);
+      bool ohas = __shfl_xor_sync(0xffffffffu, (int)has, o) != 0;
+      if (ohas) acc = has ? ((lane & o) ? gsum(oacc, acc) : gsum(acc, oacc)) : oacc;
+      has = has || ohas;
+    }
+    if (lane == 0) a.gather_res[v] = has ? acc : G();
+  }
+}
+
+// ------------------------------------------------------- apply/post-apply ---
+// kernel_apply / reset_gather_result (mgpukernel/kernel.cuh:182-198, 572-607).
+template <class P>
+__global__ void __launch_bounds__(kNT) k_apply(GasArgs<P> a, int all_vertices, int has_gather) {
+  Ctl *ctl = a.ctl;
+  if (!ctl->active || ctl->mode != MODE_QUEUE) return;
+  const uint32_t level = ctl->level;
+  const uint32_t n = all_vertices ? (uint32_t)a.g.V : ctl->frontier_size;
+  const int32_t *F = cur_queue(a, level);
+  typename P::apply ap;
+  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    const int v = all_vertices ? (int)i : F[i];
+    typename P::GatherType gv = has_gather ? a.gather_res[v] : a.gather_tmp[v];
+    char ch = (char)a.changed[v];
+    ap(v, (int)level, gv, a.vl, a.el, ch);
+    a.changed[v] = (uint8_t)ch;
+  }
+}
+
+template <class P>
+__global__ void __launch_bounds__(kNT) k_post_apply(GasArgs<P> a, int all_vertices) {
+  Ctl *ctl = a.ctl;
+  if (!ctl->active || ctl->mode != MODE_QUEUE) return;
+  const uint32_t level = ctl->level;
+  const uint32_t n = all_vertices ? (uint32_t)a.g.V : ctl->frontier_size;
+  const int32_t *F = cur_queue(a, level);
+  typename P::post_apply pa;
+  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    const int v = all_vertices ? (int)i : F[i];
+    pa(v, a.vl, a.el, a.gather_tmp);
+  }
+}
+
+// ---------------------------------------------------------- frontier scan ---
+// Exclusive prefix of expanded degrees over the frontier + merge-path tile
+// partitions of the item space. Also clears the current frontier's bits in the
+// parity bitmap so it is clean when reused two levels later.
+template <class P, int VTS, int VT>
+__global__ void __launch_bounds__(kNT) k_frontier_scan(GasArgs<P> a) {
+  constexpr uint32_t TV = kNT * VTS;
+  constexpr uint32_t NV = kNT * VT;
+  __shared__ uint32_t s_red[kNW + 1];
+  __shared__ uint32_t s_tile, s_prefix;
+  __shared__ int s_fail;
+  Ctl *ctl = a.ctl;
+  if (!ctl->active || ctl->mode != MODE_QUEUE) return;
+  const uint32_t level = ctl->level, n = ctl->frontier_size, epoch = ctl->epoch;
+  const unsigned long long spin_limit = ctl->spin_limit;
+  const int32_t *F = cur_queue(a, level);
+  uint32_t *clear_bm = cur_bm(a, level);
+  const int32_t *ro = a.expand_in ? a.g.csc_offsets : a.g.row_offsets;
+  const uint32_t ntiles = (n + TV - 1) / TV;
+  typename P::expand_vertex ev;
+  if (threadIdx.x == 0) s_fail = 0;
+  for (;;) {
+    const uint32_t tile = next_tile(&ctl->tile_ctr[0], &s_tile);
+    if (tile >= ntiles || s_fail) break;
+    const uint32_t ib = tile * TV + threadIdx.x * VTS;
+    uint32_t deg[VTS];
+    uint32_t tsum = 0;
+#pragma unroll
+    for (int k = 0; k < VTS; ++k) {
+      const uint32_t i = ib + k;
+      uint32_t d = 0;
+      if (i < n) {
+        const int v = F[i];
+        atomicAnd(&clear_bm[v >> 5], ~(1u << (v & 31)));
+        bool expand = true;
+        if (skip_unchanged_trait<P>::value) expand = ev(v, (char)a.changed[v], a.vl, a.el);
+        d = expand ? (uint32_t)(ro[v + 1] - ro[v]) : 0u;
+      }
+      deg[k] = d;
+      tsum += d;
+    }
+    uint32_t tile_total;
+    const uint32_t excl = cta_exclusive_sum(tsum, s_red, &tile_total);
+    if (warp_id() == 0) {
+      bool failed = false;
+      const uint32_t pre = lookback(a.status, tile, tile_total, epoch, spin_limit, &failed);
+      if (lane_id() == 0) {
+        s_prefix = pre;
+        if (failed) {
+          s_fail = 1;
+          raise_error(ctl, MG_ERR_TIMEOUT);
+        } else if (tile == ntiles - 1) {
+          const uint32_t total = pre + tile_total;
+          ctl->edge_total = total;
+          ctl->exp_tiles = (uint32_t)(((unsigned long long)n + total + NV - 1) / NV);
+        }
+      }
+    }
+    __syncthreads();
+    if (s_fail) break;
+    uint32_t run = s_prefix + excl;
+#pragma unroll
+    for (int k = 0; k < VTS; ++k) {
+      const uint32_t i = ib + k;
+      if (i < n) {
+        a.scan[i] = run;
+        const unsigned long long base = (unsigned long long)i + run;
+        const uint32_t t0 = (uint32_t)((base + NV - 1) / NV);
+        const uint32_t t1 = (uint32_t)((base + deg[k]) / NV);
+        for (uint32_t t = t0; t <= t1; ++t) a.part[t] = (int32_t)i;
+        run += deg[k];
+      }
+    }
+  }
+}
+
+// ------------------------------------------------------ expand + contract ---
+template <class P, int VT>
+__global__ void __launch_bounds__(kNT) k_expand(GasArgs<P> a) {
+  constexpr int NV = kNT * VT;
+  __shared__ int32_t s_v[NV + 1];
+  __shared__ int32_t s_base[NV + 1];
+  __shared__ int32_t s_rs[NV + 1];
+  __shared__ int32_t s_own[NV];
+  __shared__ uint8_t s_ch[NV + 1];
+  __shared__ uint32_t s_cnt[VT * kNW + 1];
+  __shared__ uint32_t s_tile, s_prefix, s_warpmax[kNW];
+  __shared__ int s_fail;
+  __shared__ unsigned long long s_edges;
+  Ctl *ctl = a.ctl;
+  if (!ctl->active || ctl->mode != MODE_QUEUE) return;
+  const uint32_t level = ctl->level, n = ctl->frontier_size, total = ctl->edge_total;
+  const uint32_t ntiles = ctl->exp_tiles, epoch = ctl->epoch + 1;
+  const unsigned long long spin_limit = ctl->spin_limit;
+  const unsigned long long items = (unsigned long long)n + total;
+  const int32_t *F = cur_queue(a, level);
+  int32_t *Fout = nxt_queue(a, level);
+  uint32_t *dedup = nxt_bm(a, level);
+  const int32_t *ro = a.expand_in ? a.g.csc_offsets : a.g.row_offsets;
+  const int32_t *nb = a.expand_in ? a.g.csc_rows : a.g.col;
+  const int32_t V = a.g.V;
+  typename P::expand_vertex ev;
+  typename P::expand_edge ee;
+  typename P::contract ct;
+  const int lane = lane_id(), warp = warp_id();
+  unsigned long long my_edges = 0;
+  if (threadIdx.x == 0) {
+    s_fail = 0;
+    s_edges = 0;
+  }
+  for (;;) {
+    const uint32_t tile = next_tile(&ctl->tile_ctr[1], &s_tile);
+    if (tile >= ntiles || s_fail) break;
+    const unsigned long long d0 = (unsigned long long)tile * NV;
+    const int cnt = (int)((items - d0) < (unsigned long long)NV ? (items - d0) : (unsigned long long)NV);
+    const int i0 = a.part[tile];
+    int i1 = (tile + 1 < ntiles) ? a.part[tile + 1] : (int)n - 1;
+    if (i1 > (int)n - 1) i1 = (int)n - 1;
+    const int nblk = i1 - i0 + 1;
+    if (nblk < 1 || nblk > NV + 1 || i0 < 0) {
+      // Inconsistent partition (cannot happen for a well-formed scan): record
+      // it and stop instead of indexing out of bounds.
+      if (threadIdx.x == 0) {
+        raise_error(ctl, MG_ERR_OVERFLOW);
+        s_fail = 1;
+      }
+      __syncthreads();
+      break;
+    }
+    for (int j = threadIdx.x; j < nblk; j += kNT) {
+      const int i = i0 + j;
+      const int v = F[i];
+      s_v[j] = v;
+      s_base[j] = (int32_t)((long long)i + (long long)a.scan[i] - (long long)d0);
+      s_rs[j] = ro[v];
+      s_ch[j] = (uint8_t)ev(v, (char)a.changed[v], a.vl, a.el);
+    }
+    for (int k = threadIdx.x; k < NV; k += kNT) s_own[k] = 0;
+    __syncthreads();
+    for (int j = 1 + threadIdx.x; j < nblk; j += kNT) {
+      const int b = s_base[j];
+      if (b >= 0 && b < cnt) s_own[b] = j;
+    }
+    __syncthreads();
+    // Inclusive max-scan of owner markers: VT consecutive entries per thread.
+    {
+      int loc[VT];
+      int m = 0;
+#pragma unroll
+      for (int r = 0; r < VT; ++r) {
+        int x = s_own[threadIdx.x * VT + r];
+        m = x > m ? x : m;
+        loc[r] = m;
+      }
+      int wm = m;
+#pragma unroll
+      for (int o = 1; o < 32; o <<= 1) {
+        int y = __shfl_up_sync(0xffffffffu, wm, o);
+        if (lane >= o) wm = y > wm ? y : wm;
+      }
+      if (lane == 31) s_warpmax[warp] = (uint32_t)wm;
+      __syncthreads();
+      int carry = 0;
+      for (int w = 0; w < warp; ++w) carry = (int)s_warpmax[w] > carry ? (int)s_warpmax[w] : carry;
+      int prev = __shfl_up_sync(0xffffffffu, wm, 1);
+      if (lane > 0) carry = prev > carry ? prev : carry;
+#pragma unroll
+      for (int r = 0; r < VT; ++r) s_own[threadIdx.x * VT + r] = loc[r] > carry ? loc[r] : carry;
+    }
+    __syncthreads();
+    uint32_t bal[VT];
+    int32_t outv[VT];
+#pragma unroll
+    for (int r = 0; r < VT; ++r) {
+      const int k = r * kNT + threadIdx.x;
+      bool surv = false;
+      int fo = -1;
+      if (k < cnt) {
+        const int j = s_own[k];
+        const int el = k - s_base[j] - 1;
+        if (el >= 0) {
+          const int v = s_v[j];
+          const int eid = s_rs[j] + el;
+          if ((unsigned)eid < (unsigned)a.g.E) {
+            const int nbr = nb[eid];
+            const int eidv = (a.expand_in && a.g.csc_eid) ? a.g.csc_eid[eid] : eid;
+            typename P::MiscType misc = typename P::MiscType();
+            ee(s_ch[j] != 0, (int)level, v, nbr, eidv, a.vl, a.el, fo, misc);
+            if (fo >= V) {
+              raise_error(ctl, MG_ERR_OVERFLOW);
+              fo = -1;
+            }
+            if (fo >= 0) ct((int)level, fo, a.vl, a.el, a.gather_tmp, misc);
+            if (fo >= V) {
+              raise_error(ctl, MG_ERR_OVERFLOW);
+              fo = -1;
+            }
+          } else {
+            raise_error(ctl, MG_ERR_OVERFLOW);
+          }
+          if (fo >= 0) {
+            const uint32_t bit = 1u << (fo & 31);
+            uint32_t *w = dedup + (fo >> 5);
+            if (!(ld_volatile(w) & bit)) surv = !(atomicOr(w, bit) & bit);
+          }
+          if (track_next_edges_trait<P>::value && surv) my_edges += (unsigned long long)(ro[fo + 1] - ro[fo]);
+        }
+      }
+      bal[r] = __ballot_sync(0xffffffffu, surv);
+      outv[r] = fo;
+      if (lane == 0) s_cnt[r * kNW + warp] = __popc(bal[r]);
+    }
+    __syncthreads();
+    if (warp == 0) {
+      // Exclusive scan over the VT*kNW (round, warp) counts; 2 per lane for VT*kNW <= 64.
+      constexpr int C = VT * kNW;
+      constexpr int PER = (C + 31) / 32;
+      uint32_t x[PER];
+      uint32_t s = 0;
+#pragma unroll
+      for (int q = 0; q < PER; ++q) {
+        const int idx = lane * PER + q;
+        x[q] = idx < C ? s_cnt[idx] : 0u;
+        s += x[q];
+      }
+      const uint32_t inc = warp_inclusive_sum(s);
+      uint32_t run = inc - s;
+#pragma unroll
+      for (int q = 0; q < PER; ++q) {
+        const int idx = lane * PER + q;
+        if (idx < C) s_cnt[idx] = run;
+        run += x[q];
+      }
+      const uint32_t tile_total = __shfl_sync(0xffffffffu, inc, 31);
+      bool failed = false;
+      const uint32_t pre = lookback(a.status, tile, tile_total, epoch, spin_limit, &failed);
+      if (lane == 0) {
+        s_prefix = pre;
+        if (failed) {
+          s_fail = 1;
+          raise_error(ctl, MG_ERR_TIMEOUT);
+        } else if (tile == ntiles - 1) {
+          ctl->next_size = pre + tile_total;
+        }
+      }
+    }
+    __syncthreads();
+    if (s_fail) break;
+#pragma unroll
+    for (int r = 0; r < VT; ++r) {
+      if ((bal[r] >> lane) & 1u) {
+        const uint32_t pos = s_prefix + s_cnt[r * kNW + warp] + __popc(bal[r] & lanemask_lt());
+        if (pos < (uint32_t)V) Fout[pos] = outv[r];
+      }
+    }
+  }
+  if (track_next_edges_trait<P>::value) {
+    my_edges = warp_sum(my_edges);
+    if (lane == 0 && my_edges) atomicAdd(&s_edges, my_edges);
+    __syncthreads();
+    if (threadIdx.x == 0 && s_edges) atomicAdd(&ctl->next_edges, s_edges);
+  }
+}
+
+// ---------------------------------------------------------------- level end -
+// Advances the level and decides whether the loop continues; inside a CUDA
+// graph it drives the WHILE node's condition.
+__global__ void k_level_end(Ctl *ctl, cudaGraphConditionalHandle h, int use_handle);
+
+// --------------------------------------------------------------- utilities --
+__global__ void k_fill_i32(int32_t *p, int32_t v, int64_t n);
+__global__ void k_sequence_i32(int32_t *p, int64_t n);
+__global__ void k_ctl_init(Ctl *ctl, uint32_t frontier_size, uint32_t max_iter, unsigned long long spin_limit,
+                           uint32_t mode);
+
+}  // namespace mg

@@ -1,0 +1,103 @@
+// Device-resident graph (the B200 counterpart of CsrProblem::GraphSlice,
+// GASengine/csr_problem.cuh:150-354) and its working set.
+//
+// HBM layout, all int32 unless noted, every array 256-byte aligned:
+//   row_offsets[V+1+pad]  CSR offsets (padded to a multiple of 4 entries + 4 so
+//                         16-byte bulk copies of any aligned 4-entry tile stay in bounds)
+//   col[E+pad]            CSR column indices
+//   wgt[E]                int32 edge values (SSSP weights), optional
+//   csc_offsets/csc_rows  transposed graph (in-edges); aliases the CSR when the
+//                         graph is symmetric
+//   csc_eid[E]            CSR edge id of every CSC entry (pull access to edge values)
+//   out_degree_inv[V]     float 1/outdeg (PageRank), built on first use
+// The working set (queues, scan buffers, bitmaps, look-back status words) is
+// allocated once per graph and reused by every run on it.
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include <map>
+#include <string>
+#include <vector>
+
+#include "common.cuh"
+
+namespace mg {
+
+struct DevCsr {
+  int32_t *row_offsets = nullptr;
+  int32_t *col = nullptr;
+  int32_t *wgt = nullptr;
+  int32_t *csc_offsets = nullptr;
+  int32_t *csc_rows = nullptr;
+  int32_t *csc_eid = nullptr;
+  int32_t V = 0;
+  int32_t E = 0;
+};
+
+// Working set shared by the level-loop kernels (sizes in elements).
+struct Workspace {
+  int32_t *queue[2] = {nullptr, nullptr};  // frontier ping-pong, capacity V
+  uint32_t *scan = nullptr;                // degree prefix of the frontier, V+1
+  int32_t *part = nullptr;                 // expand tile -> first frontier index
+  unsigned long long *status = nullptr;    // look-back status words
+  uint32_t *bm[2] = {nullptr, nullptr};    // frontier bitmaps (level parity), V/32+1 words
+  uint32_t *visited = nullptr;             // visited bitmap, V/32+1 words
+  uint8_t *changed = nullptr;              // apply() change flags, V
+  int32_t *gather_tmp = nullptr;           // contract/gather scratch (4-byte GatherType), V
+  int32_t *vbuf[2] = {nullptr, nullptr};   // program vertex arrays (labels, dists, dists_out)
+  Ctl *ctl = nullptr;
+  size_t part_cap = 0;
+  size_t status_cap = 0;
+  size_t words = 0;
+  size_t bytes = 0;
+};
+
+}  // namespace mg
+
+namespace mg {
+// An instantiated level loop (CUDA graph with a WHILE node), cached per graph
+// and per loop body so repeated runs only pay cudaGraphLaunch.
+struct LoopCache {
+  cudaGraph_t graph = nullptr;
+  cudaGraphExec_t exec = nullptr;
+  int kernels_per_level = 0;
+};
+}  // namespace mg
+
+struct mg_graph {
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+  mg::Ctl *host_ctl = nullptr;  // pinned copy of the control block
+  std::map<std::string, mg::LoopCache> loops;
+  int num_sms = 148;
+  int directed = 0;
+  int64_t nodes = 0;
+  int64_t edges = 0;
+  mg::DevCsr csr;
+  std::vector<int64_t> graph_offsets;  // batch of graphs: first vertex of each graph
+  mg::Workspace ws;
+  float *inv_outdeg = nullptr;          // PageRank 1/outdeg (0 for dangling vertices)
+  uint8_t *dangling_flags = nullptr;
+  int32_t *ref_outdeg = nullptr;        // reference PageRank out-degree (PageRank.h:141-161)
+  // Batched (mask-frontier) working set, allocated on first use.
+  unsigned long long *mask[3] = {nullptr, nullptr, nullptr};
+  int32_t *multi_out = nullptr;         // [V][64] int32 per-source results
+  size_t multi_bytes = 0;
+  size_t device_bytes = 0;
+  uint64_t epochs_used = 0;  // look-back epochs consumed since the status words were cleared
+  std::vector<void *> allocations;
+};
+
+namespace mg {
+
+// Library-internal helpers implemented in graph.cu.
+int device_alloc(mg_graph *g, void **p, size_t bytes);
+int ensure_workspace(mg_graph *g);
+int ensure_multi(mg_graph *g, bool need_dist);
+cudaStream_t run_stream(mg_graph *g, const mg_options *o);
+int cuda_status(cudaError_t e, const char *what);
+int launch_check(const char *what);
+
+}  // namespace mg

@@ -1,0 +1,23 @@
+// Entry points whose kernels live in translation units that are not built yet.
+#include "graph.cuh"
+#include "host_util.h"
+
+extern "C" {
+
+int mg_bfs_multi(mg_graph *, const int32_t *, int32_t, int32_t *, mg_stats *, const mg_options *) {
+  return mg::set_error(MG_ERR_UNSUPPORTED, "mg_bfs_multi not built");
+}
+int mg_sssp_multi(mg_graph *, const int32_t *, int32_t, int32_t *, mg_stats *, const mg_options *) {
+  return mg::set_error(MG_ERR_UNSUPPORTED, "mg_sssp_multi not built");
+}
+int mg_pagerank(mg_graph *, float *, mg_stats *, const mg_options *) {
+  return mg::set_error(MG_ERR_UNSUPPORTED, "mg_pagerank not built");
+}
+int mg_ppr_forward(mg_graph *, const float *, const float *, int32_t, float *, mg_stats *, const mg_options *) {
+  return mg::set_error(MG_ERR_UNSUPPORTED, "mg_ppr_forward not built");
+}
+int mg_ppr_backward(mg_graph *, const float *, const float *, const float *, int32_t, float *, float *, mg_stats *,
+                    const mg_options *) {
+  return mg::set_error(MG_ERR_UNSUPPORTED, "mg_ppr_backward not built");
+}
+}
