@@ -1,0 +1,386 @@
+"""Benchmark of the B200 GAS hot path (one JSON line on rank 0).
+
+Workload (R-MAT scale 22, edgefactor 16, A/B/C/D = .57/.19/.19/.05, seed 1,
+symmetrised, self-loops and duplicates removed, int32 CSR; uint32 weights in
+[1, 64]): a step is one batched BFS from 64 seeded sources (the 64-bit mask
+frontier, mg_bfs_multi). value = aggregate GTEPS = sum over sources of the
+out-degrees of the vertices each source reaches, divided by the step time.
+Alongside, in sub_results: the same 64 sources as 64 sequential single-source
+BFS runs (the "plain engine"), 8 single-source SSSP runs, batched 64-source
+SSSP, CC, and the reference PageRank program.
+
+--impl reference times the reference's own CPU BFS (CPUBFS, compiled from the
+reference sources into oracle/_ref, or the oracle restatement when that is
+absent) on the same graph and sources, one source per host core.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import threading
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+SCALE, EDGEFACTOR, SEED = 22, 16, 1
+NSRC = 64
+WORKLOAD = (f"R-MAT scale {SCALE} edgefactor {EDGEFACTOR} A/B/C/D .57/.19/.19/.05 seed {SEED}, symmetrised, "
+            f"cleaned, int32 CSR; batched BFS from {NSRC} seeded sources (64-bit mask frontier)")
+
+
+def log(*a):
+    print(*a, file=sys.stderr, flush=True)
+
+
+def pick_sources(hg, n, seed=SEED):
+    rng = np.random.default_rng(seed)
+    cand = np.flatnonzero(np.diff(hg.row_offsets) > 0)
+    return np.sort(rng.choice(cand, size=n, replace=False)).astype(np.int32)
+
+
+def edges_reached(hg, depths_row_or_oracle):
+    deg = np.diff(hg.row_offsets).astype(np.int64)
+    return int(deg[depths_row_or_oracle >= 0].sum())
+
+
+# ------------------------------------------------------------------ clocks --
+class ClockSampler:
+    QUERY = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device_index: int = 0):
+        self.dev = device_index
+        self.proc = None
+        self.lines: list[str] = []
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.dev}", f"--query-gpu={self.QUERY}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except Exception:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def __exit__(self, *exc):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+
+    def summary(self) -> dict:
+        sm, mx, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            f = [x.strip() for x in ln.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                mx.append(float(f[2]))
+            except ValueError:
+                continue
+            for n, v in zip(names, f[5:9]):
+                if v.lower() == "active":
+                    reasons.add(n)
+        if not sm:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": max(mx), "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def measured_peak_hbm():
+    p = ROOT / "MEASURED_PEAKS.json"
+    if p.exists():
+        try:
+            return float(json.loads(p.read_text())["hbm_gbs"]), "measured"
+        except Exception:
+            pass
+    return 6650.0, "fallback"
+
+
+# ------------------------------------------------------------- native arm --
+def run_native(args, rank: int, world: int):
+    import torch
+
+    import gpugraph_b200 as gg
+    from gpugraph_b200 import _lib
+
+    lib = _lib.lib
+    torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
+    t0 = time.time()
+    hg = gg.HostGraph.rmat(args.scale, EDGEFACTOR, seed=SEED).with_weights(1, 64, seed=SEED)
+    log(f"[bench] graph V={hg.nodes} E={hg.edges} built in {time.time() - t0:.1f}s")
+    srcs = pick_sources(hg, NSRC)
+    g = gg.Graph(hg)
+    dev = torch.device("cuda")
+    out_dev = torch.empty((NSRC, hg.nodes), dtype=torch.int32, device=dev)
+    stream = torch.cuda.current_stream()
+    base_opts = dict(outputs_on_device=1, stream=stream.cuda_stream, compute_stats=0)
+    o_multi = _lib.default_options(**base_opts)
+    st = _lib.Stats()
+    src_arr = np.ascontiguousarray(srcs)
+
+    def multi_step(opts=o_multi):
+        _lib.check(lib.mg_bfs_multi(g.handle, src_arr.ctypes.data, NSRC, out_dev.data_ptr(), None, opts),
+                   "mg_bfs_multi")
+
+    # TEPS numerator (once, outside timing), and parity spot-check on rank 0
+    o_stats = _lib.default_options(**dict(base_opts, compute_stats=1))
+    _lib.check(lib.mg_bfs_multi(g.handle, src_arr.ctypes.data, NSRC, out_dev.data_ptr(), st, o_stats), "stats")
+    teps_edges = int(st.edges_traversed)
+    levels_multi = (st.iterations, st.push_iterations, st.pull_iterations)
+
+    for _ in range(args.warmup):
+        multi_step()
+    torch.cuda.synchronize()
+    lib.mg_kernel_launches(1)
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with ClockSampler(torch.cuda.current_device()) as clk:
+        if world > 1:
+            torch.distributed.barrier()
+        torch.cuda.synchronize()
+        ev0.record(stream)
+        for _ in range(args.steps):
+            multi_step()
+        ev1.record(stream)
+        torch.cuda.synchronize()
+        if world > 1:
+            torch.distributed.barrier()
+    launches = int(lib.mg_kernel_launches(1))
+    ms_step = ev0.elapsed_time(ev1) / args.steps
+    if world > 1:
+        t = torch.tensor([ms_step], device=dev)
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+        ms_step = float(t.item())
+    value = world * teps_edges / (ms_step * 1e-3) / 1e9
+
+    # ---- plain engine: the same sources one at a time
+    o_single = _lib.default_options(**base_opts)
+    one = torch.empty(hg.nodes, dtype=torch.int32, device=dev)
+    for s in srcs[:4]:
+        _lib.check(lib.mg_bfs(g.handle, int(s), one.data_ptr(), None, o_single), "mg_bfs")
+    torch.cuda.synchronize()
+    ev0.record(stream)
+    for s in srcs:
+        _lib.check(lib.mg_bfs(g.handle, int(s), one.data_ptr(), None, o_single), "mg_bfs")
+    ev1.record(stream)
+    torch.cuda.synchronize()
+    single_ms = ev0.elapsed_time(ev1)
+    single_gteps = teps_edges / (single_ms * 1e-3) / 1e9
+
+    # ---- parity spot check of the batched result against single-source runs
+    parity = True
+    for k in (0, NSRC // 2, NSRC - 1):
+        _lib.check(lib.mg_bfs(g.handle, int(srcs[k]), one.data_ptr(), None, o_single), "mg_bfs")
+        parity &= bool(torch.equal(one, out_dev[k]))
+
+    sub = {"bfs_batched64": {"gteps": value / world, "ms": ms_step, "levels": levels_multi},
+           "bfs_single_x64": {"gteps": single_gteps, "ms_total": single_ms, "ms_per_source": single_ms / NSRC},
+           "batched_over_single": value / world / single_gteps,
+           "batched_equals_single_spot_check": parity}
+
+    # ---- SSSP: 8 sources one at a time (plain), and batched 64
+    if not args.quick:
+        o_s = _lib.default_options(**dict(base_opts, compute_stats=1))
+        sssp_edges, sssp_ms = 0, 0.0
+        for s in srcs[:8]:
+            _lib.check(lib.mg_sssp(g.handle, int(s), one.data_ptr(), st, o_s), "mg_sssp")
+            sssp_edges += int(st.edges_traversed)
+            sssp_ms += float(st.device_ms)
+        sub["sssp_single_x8"] = {"gteps": sssp_edges / (sssp_ms * 1e-3) / 1e9, "ms_per_source": sssp_ms / 8}
+        try:
+            _lib.check(lib.mg_sssp_multi(g.handle, src_arr.ctypes.data, NSRC, out_dev.data_ptr(), st, o_s),
+                       "mg_sssp_multi")
+            ev0.record(stream)
+            _lib.check(lib.mg_sssp_multi(g.handle, src_arr.ctypes.data, NSRC, out_dev.data_ptr(), None, o_multi),
+                       "mg_sssp_multi")
+            ev1.record(stream)
+            torch.cuda.synchronize()
+            mms = ev0.elapsed_time(ev1)
+            sub["sssp_batched64"] = {"gteps": int(st.edges_traversed) / (mms * 1e-3) / 1e9, "ms": mms,
+                                     "levels": int(st.iterations),
+                                     "over_single": (int(st.edges_traversed) / mms) / (sssp_edges / sssp_ms)}
+        except Exception as e:  # noqa: BLE001
+            sub["sssp_batched64"] = {"error": str(e)[:200]}
+        lab = torch.empty(hg.nodes, dtype=torch.int32, device=dev)
+        _lib.check(lib.mg_cc(g.handle, lab.data_ptr(), st, o_multi), "mg_cc")
+        ev0.record(stream)
+        _lib.check(lib.mg_cc(g.handle, lab.data_ptr(), st, o_multi), "mg_cc")
+        ev1.record(stream)
+        torch.cuda.synchronize()
+        cms = ev0.elapsed_time(ev1)
+        sub["cc"] = {"gedges_per_s": hg.edges / (cms * 1e-3) / 1e9, "ms": cms, "iterations": int(st.iterations)}
+
+    # ---- end to end through the C ABI with host buffers (pinned), one call per step
+    host_out = torch.empty((NSRC, hg.nodes), dtype=torch.int32, pin_memory=True)
+    o_host = _lib.default_options(stream=stream.cuda_stream, compute_stats=0)
+    src_pinned = torch.from_numpy(src_arr.copy()).pin_memory()
+    _lib.check(lib.mg_bfs_multi(g.handle, src_pinned.data_ptr(), NSRC, host_out.data_ptr(), None, o_host), "e2e")
+    torch.cuda.synchronize()
+    e2e_steps = max(1, min(args.steps, 5))
+    t1 = time.perf_counter()
+    for _ in range(e2e_steps):
+        _lib.check(lib.mg_bfs_multi(g.handle, src_pinned.data_ptr(), NSRC, host_out.data_ptr(), None, o_host), "e2e")
+    e2e_s = (time.perf_counter() - t1) / e2e_steps
+    e2e = {"value": world * teps_edges / e2e_s / 1e9, "unit": "GTEPS", "h2d_bytes_per_step": NSRC * 4,
+           "d2h_bytes_per_step": NSRC * hg.nodes * 4, "ms_per_step": e2e_s * 1e3}
+
+    # ---- live roofline of the dominant kernel (profiled pass, host-driven loop)
+    lib.mg_profile_enable(1)
+    multi_step()
+    torch.cuda.synchronize()
+    prof = _lib.profile_read()
+    lib.mg_profile_enable(0)
+    kernels = {k: v for k, v in prof.items() if k != "other"}
+    dom = max(kernels, key=lambda k: kernels[k][0]) if kernels else None
+    peak, peak_kind = measured_peak_hbm()
+    roofline = None
+    if dom:
+        ms, n, byts = kernels[dom]
+        achieved = byts / (ms * 1e-3) / 1e9 if ms > 0 else 0.0
+        roofline = {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak, "unit": "GB/s",
+                    "frac": achieved / peak, "traffic": None, "peak_source": peak_kind,
+                    "launches": n, "bytes_per_launch": byts / max(n, 1), "ms_per_launch": ms / max(n, 1),
+                    "kernels": {k: {"ms": v[0], "launches": v[1], "GB": v[2] / 1e9} for k, v in prof.items()}}
+
+    res = {"value": value, "ms_per_step": ms_step, "launches": launches, "sub": sub, "e2e": e2e,
+           "roofline": roofline, "clocks": clk.summary(), "V": hg.nodes, "E": hg.edges, "teps_edges": teps_edges}
+    g.close()
+    return res, hg, srcs
+
+
+# ---------------------------------------------------------- reference arm --
+def _ref_worker(args):
+    path_ro, path_col, src, use_ref = args
+    import oracle
+
+    ro = np.load(path_ro, mmap_mode="r")
+    col = np.load(path_col, mmap_mode="r")
+    t = time.perf_counter()
+    d = oracle.ref_bfs(ro, col, src) if use_ref else oracle.bfs(ro, col, src)
+    return time.perf_counter() - t, d
+
+
+def cpu_bfs_sample(hg, srcs, cores: int):
+    """Times the reference CPU BFS on `cores` sources, one per process (spawned)."""
+    import multiprocessing as mp
+
+    import oracle
+
+    use_ref = oracle.ref() is not None
+    tmp = Path(tempfile.mkdtemp(prefix="mgbench_"))
+    pro, pcol = tmp / "ro.npy", tmp / "col.npy"
+    np.save(pro, hg.row_offsets)
+    np.save(pcol, hg.column_indices)
+    sample = [int(s) for s in srcs[:cores]]
+    ctx = mp.get_context("spawn")
+    t0 = time.perf_counter()
+    with ctx.Pool(len(sample)) as pool:
+        outs = pool.map(_ref_worker, [(str(pro), str(pcol), s, use_ref) for s in sample])
+    wall = time.perf_counter() - t0
+    edges = sum(edges_reached(hg, d) for _, d in outs)
+    per_src = [t for t, _ in outs]
+    for p in (pro, pcol):
+        p.unlink()
+    tmp.rmdir()
+    return {"edges": edges, "wall_s": wall, "per_source_s": per_src, "kind": "reference" if use_ref else "port",
+            "sources": len(sample)}
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="native", choices=["native", "reference"])
+    ap.add_argument("--scale", type=int, default=SCALE)
+    ap.add_argument("--quick", action="store_true", help="skip the SSSP/CC sub-results")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    cores = len(os.sched_getaffinity(0))
+    config = {"workload": WORKLOAD.replace(f"scale {SCALE}", f"scale {args.scale}"), "nsrc": NSRC,
+              "l2": "inputs larger than L2 (CSR > 0.5 GB, per-source state 1 GB)",
+              "parallelism": f"replicas x{world}" if world > 1 else "single GPU"}
+
+    if args.impl == "reference":
+        if rank != 0:
+            return
+        import gpugraph_b200 as gg  # host builder only (same bytes as the native arm)
+
+        hg = gg.HostGraph.rmat(args.scale, EDGEFACTOR, seed=SEED)
+        srcs = pick_sources(hg, NSRC)
+        ncores = max(1, min(cores, NSRC))
+        for _ in range(args.warmup):
+            pass  # the CPU code has no warm-up state; the steps below are all timed
+        vals = []
+        last = None
+        for _ in range(max(1, args.steps)):
+            last = cpu_bfs_sample(hg, np.roll(srcs, -len(vals) * ncores), ncores)
+            vals.append(last["edges"] / last["wall_s"] / 1e9)
+        v = statistics.median(vals)
+        line = {"impl": "reference", "metric": "BFS aggregate GTEPS (64 sources, R-MAT scale 22)", "value": v,
+                "unit": "GTEPS", "n_gpus": 0, "steps": args.steps, "warmup": args.warmup, "higher_is_better": True,
+                "dtype": "int32", "data": "synthetic", "config": config,
+                "cpu_baseline": {"value": v, "unit": "GTEPS", "cores": ncores, "kind": last["kind"],
+                                 "sample": f"{ncores} of the 64 sources per step, one CPUBFS per core "
+                                           f"(spawned processes), wall time per step"},
+                "e2e": {"value": v, "unit": "GTEPS", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+        print(json.dumps(line), flush=True)
+        return
+
+    if world > 1:
+        import torch
+
+        torch.distributed.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=120))
+    res, hg, srcs = run_native(args, rank, world)
+    if rank != 0:
+        if world > 1:
+            import torch
+
+            torch.distributed.destroy_process_group()
+        return
+    cpu = None
+    if not args.no_cpu_baseline:
+        n = max(1, min(4, cores))
+        c = cpu_bfs_sample(hg, srcs, n)
+        cpu = {"value": c["edges"] / c["wall_s"] / 1e9, "unit": "GTEPS", "cores": n, "kind": c["kind"],
+               "sample": f"CPUBFS from {n} of the 64 sources, one process per core, wall {c['wall_s']:.1f}s"}
+    line = {
+        "metric": "BFS aggregate GTEPS, batched 64-source (mask frontier) on R-MAT scale 22",
+        "value": res["value"], "unit": "GTEPS", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": res["ms_per_step"], "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "int32", "data": "synthetic", "config": config,
+        "e2e": res["e2e"], "roofline": res["roofline"], "cpu_baseline": cpu, "gpu_launches": res["launches"],
+        "clocks": res["clocks"], "sub_results": res["sub"],
+        "graph": {"V": res["V"], "E": res["E"], "teps_edges_per_step": res["teps_edges"]},
+    }
+    print(json.dumps(line), flush=True)
+    if world > 1:
+        import torch
+
+        torch.distributed.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

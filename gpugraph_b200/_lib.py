@@ -78,6 +78,9 @@ SIGNATURES = {
     "mg_status_string": (C.c_char_p, [C.c_int]),
     "mg_abi_version": (C.c_int, []),
     "mg_kernel_launches": (C.c_int64, [C.c_int]),
+    "mg_profile_enable": (C.c_int, [C.c_int]),
+    "mg_profile_read": (C.c_int, [C.c_int32, C.POINTER(C.c_char_p), C.POINTER(C.c_double), C.POINTER(C.c_int64),
+                                  C.POINTER(C.c_uint64)]),
     "mg_graph_create": (C.c_int, [P, P, P, C.c_int32, C.c_int64, C.c_int64, C.c_int32, OPTP, C.POINTER(P)]),
     "mg_graph_create_batch": (C.c_int, [P, P, C.c_int64, C.c_int64, P, C.c_int32, OPTP, C.POINTER(P)]),
     "mg_graph_destroy": (C.c_int, [P]),
@@ -130,6 +133,17 @@ class MapGraphError(RuntimeError):
 def check(status: int, where: str) -> None:
     if status != MG_OK:
         raise MapGraphError(status, where)
+
+
+def profile_read() -> dict:
+    """Per-kernel profile accumulated since mg_profile_enable(1): name -> (ms, launches, bytes)."""
+    out = {}
+    for k in range(12):
+        name, ms, n, b = C.c_char_p(), C.c_double(), C.c_int64(), C.c_uint64()
+        check(lib.mg_profile_read(k, C.byref(name), C.byref(ms), C.byref(n), C.byref(b)), "mg_profile_read")
+        if n.value:
+            out[name.value.decode()] = (ms.value, n.value, b.value)
+    return out
 
 
 def default_options(**kw) -> Options:

@@ -41,7 +41,7 @@ __global__ void __launch_bounds__(kNT) k_bfs_pull(GasArgs<BfsP> a) {
     s_edges = 0;
   }
   __syncthreads();
-  unsigned long long my_cnt = 0, my_edges = 0;
+  unsigned long long my_cnt = 0, my_edges = 0, my_bytes = 0;
   const uint32_t nwarps = gridDim.x * kNW;
   for (uint32_t w = blockIdx.x * kNW + warp_id(); w < words; w += nwarps) {
     const uint32_t vis = visited[w];
@@ -49,13 +49,16 @@ __global__ void __launch_bounds__(kNT) k_bfs_pull(GasArgs<BfsP> a) {
     bool found = false;
     if (v < V && !((vis >> lane) & 1u)) {
       const int beg = coff[v], end = coff[v + 1];
-      for (int e = beg; e < end; ++e) {
+      int e = beg;
+      for (; e < end; ++e) {
         const int u = crow[e];
         if ((__ldg(&cur[u >> 5]) >> (u & 31)) & 1u) {
           found = true;
           break;
         }
       }
+      // offsets + per inspected edge: row index and frontier-bitmap word
+      my_bytes += 8 + 8ull * (unsigned long long)(e - beg + (found ? 1 : 0));
     }
     const uint32_t bal = __ballot_sync(0xffffffffu, found);
     if (lane == 0) {
@@ -63,11 +66,14 @@ __global__ void __launch_bounds__(kNT) k_bfs_pull(GasArgs<BfsP> a) {
       if (bal) visited[w] = vis | bal;
       my_cnt += __popc(bal);
     }
+    if (lane == 0) my_bytes += 8;  // visited word + next-frontier word
     if (found) {
+      my_bytes += 4;
       a.vl.d_labels[v] = (int)level + 1;
       my_edges += (unsigned long long)(ro[v + 1] - ro[v]);
     }
   }
+  add_bytes(ctl->kbytes, KID_BFS_PULL, my_bytes);
   my_edges = warp_sum(my_edges);
   if (lane == 0) {
     if (my_cnt) atomicAdd(&s_cnt, my_cnt);
@@ -266,11 +272,11 @@ int bfs_run(mg_graph *g, const std::vector<int32_t> &roots, int32_t *depths, mg_
   const int32_t Vv = g->csr.V;
   const int64_t E = g->edges;
   LevelBody body = [=](cudaStream_t ss, cudaGraphConditionalHandle h, int use_h) {
-    k_bm_to_queue<<<grid, kNT, 0, ss>>>(a);
-    k_frontier_scan<BfsP, kVTS, kVT><<<grid, kNT, 0, ss>>>(a);
-    k_expand<BfsP, kVT><<<grid, kNT, 0, ss>>>(a);
-    k_bfs_pull<<<grid, kNT, 0, ss>>>(a);
-    k_bfs_level_end<<<1, 32, 0, ss>>>(a.ctl, Vv, E, h, use_h);
+    MG_LAUNCH(KID_CONVERT, ss, k_bm_to_queue<<<grid, kNT, 0, ss>>>(a));
+    MG_LAUNCH(KID_SCAN, ss, (k_frontier_scan<BfsP, kVTS, kVT><<<grid, kNT, 0, ss>>>(a)));
+    MG_LAUNCH(KID_EXPAND, ss, (k_expand<BfsP, kVT><<<grid, kNT, 0, ss>>>(a)));
+    MG_LAUNCH(KID_BFS_PULL, ss, k_bfs_pull<<<grid, kNT, 0, ss>>>(a));
+    MG_LAUNCH(KID_OTHER, ss, k_bfs_level_end<<<1, 32, 0, ss>>>(a.ctl, Vv, E, h, use_h));
   };
   LoopResult res;
   st = run_level_loop(g, s, "bfs/" + std::to_string(grid), 5, body, o->use_cuda_graph != 0, &res);
@@ -281,7 +287,7 @@ int bfs_run(mg_graph *g, const std::vector<int32_t> &roots, int32_t *depths, mg_
     stats->iterations = (int32_t)res.ctl.level;
     stats->push_iterations = (int32_t)res.ctl.push_levels;
     stats->pull_iterations = (int32_t)res.ctl.pull_levels;
-    stats->converged = res.ctl.active ? 0 : 1;
+    stats->converged = (res.ctl.frontier_size == 0) ? 1 : 0;
     stats->device_ms = res.ms;
     stats->vertices_reached = (int64_t)res.ctl.visited_count;
     stats->edges_traversed = 0;

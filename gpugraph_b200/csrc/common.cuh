@@ -39,6 +39,8 @@ struct Ctl {
   uint32_t pull_levels;
   uint32_t dir_policy;      // MG_DIR_* (BFS)
   uint32_t convert;         // 1: rebuild the queue from the bitmap at level start
+  uint32_t prev_size;       // |F| of the previous level (batched traversals)
+  uint32_t apply_pending;   // 1: the previous push level left bits to apply
   float alpha, beta;        // direction-switch factors (BFS)
   unsigned long long next_edges;     // sum of degrees of the next frontier
   unsigned long long visited_edges;  // sum of degrees of visited vertices (BFS)
@@ -47,7 +49,37 @@ struct Ctl {
   double residual;          // PageRank L1 residual of the last iteration
   double dangling;          // PageRank dangling mass of the current ranks
   double acc[4];            // FP64 reduction slots
+  // Algorithmic bytes moved by each kernel kind over the run (element-granular
+  // reads and writes the algorithm needs; see KernelId).
+  unsigned long long kbytes[12];
 };
+
+// Kernel kinds for per-kernel byte accounting and profiling.
+enum KernelId : int {
+  KID_SCAN = 0,
+  KID_EXPAND = 1,
+  KID_BFS_PULL = 2,
+  KID_MS_PULL = 3,
+  KID_MS_APPLY = 4,
+  KID_CONVERT = 5,
+  KID_MSS_EXPAND = 6,
+  KID_PR_PULL = 7,
+  KID_GATHER = 8,
+  KID_APPLY = 9,
+  KID_PPR = 10,
+  KID_OTHER = 11
+};
+
+// Adds a CTA's byte count to the run's counter for kernel kind `kid`
+// (one atomic per CTA; call from every thread with its own count).
+MG_DEVINL void add_bytes(unsigned long long *kbytes, int kid, unsigned long long mine) {
+  mine += __shfl_xor_sync(0xffffffffu, mine, 16);
+  mine += __shfl_xor_sync(0xffffffffu, mine, 8);
+  mine += __shfl_xor_sync(0xffffffffu, mine, 4);
+  mine += __shfl_xor_sync(0xffffffffu, mine, 2);
+  mine += __shfl_xor_sync(0xffffffffu, mine, 1);
+  if ((threadIdx.x & 31) == 0 && mine) atomicAdd(&kbytes[kid], mine);
+}
 
 MG_DEVINL uint32_t ld_acquire(const uint32_t *p) {
   uint32_t v;

@@ -1,6 +1,7 @@
 #include <cuda_runtime.h>
 
 #include <cstring>
+#include <vector>
 
 #include "../host_util.h"
 #include "driver.cuh"
@@ -61,6 +62,60 @@ int read_ctl(mg_graph *g, cudaStream_t s, Ctl *out) {
   return cuda_status(e, "control block read");
 }
 
+// ---------------------------------------------------------------- profiler --
+namespace {
+const char *kKernelNames[12] = {"frontier_scan", "expand_contract", "bfs_pull",    "multi_bfs_pull",
+                                "multi_bfs_apply", "frontier_convert", "multi_sssp_expand", "pagerank_pull",
+                                "gather",          "apply",           "ppr",               "other"};
+struct Profiler {
+  bool on = false;
+  std::vector<std::pair<int, cudaEvent_t>> marks;
+  std::vector<cudaEvent_t> pool;
+  size_t used = 0;
+  double ms[12] = {0};
+  int64_t launches[12] = {0};
+  unsigned long long bytes[12] = {0};
+  cudaEvent_t next_event() {
+    if (used == pool.size()) {
+      cudaEvent_t e;
+      cudaEventCreate(&e);
+      pool.push_back(e);
+    }
+    return pool[used++];
+  }
+};
+thread_local Profiler g_prof;
+}  // namespace
+
+bool prof_on() { return g_prof.on; }
+
+void prof_mark(cudaStream_t s, int kid) {
+  if (!g_prof.on) return;
+  cudaEvent_t e = g_prof.next_event();
+  cudaEventRecord(e, s);
+  g_prof.marks.push_back({kid, e});
+}
+
+void prof_flush(cudaStream_t s, const unsigned long long *kbytes) {
+  if (!g_prof.on) return;
+  cudaEvent_t end = g_prof.next_event();
+  cudaEventRecord(end, s);
+  cudaEventSynchronize(end);
+  for (size_t i = 0; i < g_prof.marks.size(); ++i) {
+    cudaEvent_t b = g_prof.marks[i].second;
+    cudaEvent_t e = (i + 1 < g_prof.marks.size()) ? g_prof.marks[i + 1].second : end;
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, b, e);
+    const int k = g_prof.marks[i].first;
+    g_prof.ms[k] += ms;
+    g_prof.launches[k] += 1;
+  }
+  g_prof.marks.clear();
+  g_prof.used = 0;
+  if (kbytes)
+    for (int k = 0; k < 12; ++k) g_prof.bytes[k] += kbytes[k];
+}
+
 int prepare_run(mg_graph *g, cudaStream_t s) {
   if (g->epochs_used < (1ull << 27)) return MG_OK;
   cudaError_t e = cudaMemsetAsync(g->ws.status, 0, g->ws.status_cap * 8, s);
@@ -114,7 +169,7 @@ int run_level_loop(mg_graph *g, cudaStream_t s, const std::string &key, int kern
   cudaError_t e = cudaEventRecord(g->ev0, s);
   if (e != cudaSuccess) return cuda_status(e, "event record");
   bool graphed = false;
-  if (use_graph) {
+  if (use_graph && !prof_on()) {
     auto it = g->loops.find(key);
     if (it == g->loops.end()) {
       LoopCache lc;
@@ -150,6 +205,7 @@ int run_level_loop(mg_graph *g, cudaStream_t s, const std::string &key, int kern
   if (e != cudaSuccess) return cuda_status(e, "event record");
   int st = read_ctl(g, s, &res->ctl);
   if (st != MG_OK) return st;
+  prof_flush(s, res->ctl.kbytes);
   float ms = 0.f;
   cudaEventElapsedTime(&ms, g->ev0, g->ev1);
   res->ms = ms;
@@ -159,3 +215,28 @@ int run_level_loop(mg_graph *g, cudaStream_t s, const std::string &key, int kern
 }
 
 }  // namespace mg
+
+extern "C" {
+
+int mg_profile_enable(int enable) {
+  mg::g_prof.on = enable != 0;
+  mg::g_prof.marks.clear();
+  mg::g_prof.used = 0;
+  for (int k = 0; k < 12; ++k) {
+    mg::g_prof.ms[k] = 0;
+    mg::g_prof.launches[k] = 0;
+    mg::g_prof.bytes[k] = 0;
+  }
+  return MG_OK;
+}
+
+int mg_profile_read(int32_t kind, const char **name, double *total_ms, int64_t *launches, uint64_t *bytes) {
+  if (kind < 0 || kind >= 12) return mg::set_error(MG_ERR_ARG, "kernel kind out of range");
+  if (name) *name = mg::kKernelNames[kind];
+  if (total_ms) *total_ms = mg::g_prof.ms[kind];
+  if (launches) *launches = mg::g_prof.launches[kind];
+  if (bytes) *bytes = (uint64_t)mg::g_prof.bytes[kind];
+  return MG_OK;
+}
+
+}  // extern "C"

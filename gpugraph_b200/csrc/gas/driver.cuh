@@ -44,4 +44,19 @@ int prepare_run(mg_graph *g, cudaStream_t s);
 // Called after a run with the number of levels it executed.
 void finish_run(mg_graph *g, uint32_t levels);
 
+// Per-kernel profiling (mg_profile_enable): while on, level loops run
+// host-driven and every kernel launch is bracketed by CUDA events on its
+// stream. prof_mark(s, kid) is called right before launching a kernel of kind kid.
+bool prof_on();
+void prof_mark(cudaStream_t s, int kid);
+// Closes the open interval on s, attributes the elapsed times, and adds the
+// run's device byte counters.
+void prof_flush(cudaStream_t s, const unsigned long long *kbytes);
+
+#define MG_LAUNCH(kid, stream, ...) \
+  do {                              \
+    ::mg::prof_mark(stream, kid);   \
+    __VA_ARGS__;                    \
+  } while (0)
+
 }  // namespace mg

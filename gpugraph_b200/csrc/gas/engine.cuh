@@ -48,6 +48,13 @@ template <class P>
 struct skip_unchanged_trait<P, std::void_t<decltype(P::skip_unchanged_vertices)>>
     : std::integral_constant<bool, P::skip_unchanged_vertices> {};
 
+// Bytes the Program reads per expanded edge besides the column index (its
+// status probe of the neighbour), for the algorithmic byte count; default 4.
+template <class P, class = void>
+struct probe_bytes_trait : std::integral_constant<int, 4> {};
+template <class P>
+struct probe_bytes_trait<P, std::void_t<decltype(P::probe_bytes)>> : std::integral_constant<int, P::probe_bytes> {};
+
 template <class P, class = void>
 struct track_next_edges_trait : std::false_type {};
 template <class P>
@@ -180,6 +187,7 @@ __global__ void __launch_bounds__(kNT) k_frontier_scan(GasArgs<P> a) {
   const int32_t *ro = a.expand_in ? a.g.csc_offsets : a.g.row_offsets;
   const uint32_t ntiles = (n + TV - 1) / TV;
   typename P::expand_vertex ev;
+  unsigned long long my_bytes = 0;
   if (threadIdx.x == 0) s_fail = 0;
   for (;;) {
     const uint32_t tile = next_tile(&ctl->tile_ctr[0], &s_tile);
@@ -231,9 +239,73 @@ __global__ void __launch_bounds__(kNT) k_frontier_scan(GasArgs<P> a) {
         const uint32_t t1 = (uint32_t)((base + deg[k]) / NV);
         for (uint32_t t = t0; t <= t1; ++t) a.part[t] = (int32_t)i;
         run += deg[k];
+        my_bytes += 20;  // frontier id, two row offsets, scan entry, bitmap word
       }
     }
   }
+  add_bytes(ctl->kbytes, KID_SCAN, my_bytes);
+}
+
+// ------------------------------------------------------------ tile decode --
+// Loads the frontier blocks of expand tile `tile` into shared memory and marks
+// the owner block of every item (inclusive max-scan of block start markers),
+// so item k of the tile is edge (k - s_base[s_own[k]] - 1) of vertex
+// s_v[s_own[k]] (negative: the vertex's own item). per_block(j, v) runs once per
+// loaded block. Returns false (nothing decoded) on an inconsistent partition.
+// Must be called by all kNT threads; ends with __syncthreads().
+template <int VT, class PerBlock>
+MG_DEVINL bool decode_tile(uint32_t tile, uint32_t ntiles, uint32_t n, unsigned long long items, const int32_t *part,
+                           const uint32_t *scan, const int32_t *F, const int32_t *ro, int32_t *s_v, int32_t *s_base,
+                           int32_t *s_rs, int32_t *s_own, uint32_t *s_warpmax, int *cnt_out, PerBlock per_block) {
+  constexpr int NV = kNT * VT;
+  const int lane = lane_id(), warp = warp_id();
+  const unsigned long long d0 = (unsigned long long)tile * NV;
+  const int cnt = (int)((items - d0) < (unsigned long long)NV ? (items - d0) : (unsigned long long)NV);
+  const int i0 = part[tile];
+  int i1 = (tile + 1 < ntiles) ? part[tile + 1] : (int)n - 1;
+  if (i1 > (int)n - 1) i1 = (int)n - 1;
+  const int nblk = i1 - i0 + 1;
+  *cnt_out = cnt;
+  if (nblk < 1 || nblk > NV + 1 || i0 < 0) return false;
+  for (int j = threadIdx.x; j < nblk; j += kNT) {
+    const int i = i0 + j;
+    const int v = F[i];
+    s_v[j] = v;
+    s_base[j] = (int32_t)((long long)i + (long long)scan[i] - (long long)d0);
+    s_rs[j] = ro[v];
+    per_block(j, v);
+  }
+  for (int k = threadIdx.x; k < NV; k += kNT) s_own[k] = 0;
+  __syncthreads();
+  for (int j = 1 + threadIdx.x; j < nblk; j += kNT) {
+    const int b = s_base[j];
+    if (b >= 0 && b < cnt) s_own[b] = j;
+  }
+  __syncthreads();
+  int loc[VT];
+  int m = 0;
+#pragma unroll
+  for (int r = 0; r < VT; ++r) {
+    int x = s_own[threadIdx.x * VT + r];
+    m = x > m ? x : m;
+    loc[r] = m;
+  }
+  int wm = m;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    int y = __shfl_up_sync(0xffffffffu, wm, o);
+    if (lane >= o) wm = y > wm ? y : wm;
+  }
+  if (lane == 31) s_warpmax[warp] = (uint32_t)wm;
+  __syncthreads();
+  int carry = 0;
+  for (int w = 0; w < warp; ++w) carry = (int)s_warpmax[w] > carry ? (int)s_warpmax[w] : carry;
+  int prev = __shfl_up_sync(0xffffffffu, wm, 1);
+  if (lane > 0) carry = prev > carry ? prev : carry;
+#pragma unroll
+  for (int r = 0; r < VT; ++r) s_own[threadIdx.x * VT + r] = loc[r] > carry ? loc[r] : carry;
+  __syncthreads();
+  return true;
 }
 
 // ------------------------------------------------------ expand + contract ---
@@ -265,7 +337,7 @@ __global__ void __launch_bounds__(kNT) k_expand(GasArgs<P> a) {
   typename P::expand_edge ee;
   typename P::contract ct;
   const int lane = lane_id(), warp = warp_id();
-  unsigned long long my_edges = 0;
+  unsigned long long my_edges = 0, my_bytes = 0;
   if (threadIdx.x == 0) {
     s_fail = 0;
     s_edges = 0;
@@ -274,12 +346,9 @@ __global__ void __launch_bounds__(kNT) k_expand(GasArgs<P> a) {
     const uint32_t tile = next_tile(&ctl->tile_ctr[1], &s_tile);
     if (tile >= ntiles || s_fail) break;
     const unsigned long long d0 = (unsigned long long)tile * NV;
-    const int cnt = (int)((items - d0) < (unsigned long long)NV ? (items - d0) : (unsigned long long)NV);
-    const int i0 = a.part[tile];
-    int i1 = (tile + 1 < ntiles) ? a.part[tile + 1] : (int)n - 1;
-    if (i1 > (int)n - 1) i1 = (int)n - 1;
-    const int nblk = i1 - i0 + 1;
-    if (nblk < 1 || nblk > NV + 1 || i0 < 0) {
+    int cnt;
+    if (!decode_tile<VT>(tile, ntiles, n, items, a.part, a.scan, F, ro, s_v, s_base, s_rs, s_own, s_warpmax, &cnt,
+                         [&](int j, int v) { s_ch[j] = (uint8_t)ev(v, (char)a.changed[v], a.vl, a.el); })) {
       // Inconsistent partition (cannot happen for a well-formed scan): record
       // it and stop instead of indexing out of bounds.
       if (threadIdx.x == 0) {
@@ -288,46 +357,6 @@ __global__ void __launch_bounds__(kNT) k_expand(GasArgs<P> a) {
       }
       __syncthreads();
       break;
-    }
-    for (int j = threadIdx.x; j < nblk; j += kNT) {
-      const int i = i0 + j;
-      const int v = F[i];
-      s_v[j] = v;
-      s_base[j] = (int32_t)((long long)i + (long long)a.scan[i] - (long long)d0);
-      s_rs[j] = ro[v];
-      s_ch[j] = (uint8_t)ev(v, (char)a.changed[v], a.vl, a.el);
-    }
-    for (int k = threadIdx.x; k < NV; k += kNT) s_own[k] = 0;
-    __syncthreads();
-    for (int j = 1 + threadIdx.x; j < nblk; j += kNT) {
-      const int b = s_base[j];
-      if (b >= 0 && b < cnt) s_own[b] = j;
-    }
-    __syncthreads();
-    // Inclusive max-scan of owner markers: VT consecutive entries per thread.
-    {
-      int loc[VT];
-      int m = 0;
-#pragma unroll
-      for (int r = 0; r < VT; ++r) {
-        int x = s_own[threadIdx.x * VT + r];
-        m = x > m ? x : m;
-        loc[r] = m;
-      }
-      int wm = m;
-#pragma unroll
-      for (int o = 1; o < 32; o <<= 1) {
-        int y = __shfl_up_sync(0xffffffffu, wm, o);
-        if (lane >= o) wm = y > wm ? y : wm;
-      }
-      if (lane == 31) s_warpmax[warp] = (uint32_t)wm;
-      __syncthreads();
-      int carry = 0;
-      for (int w = 0; w < warp; ++w) carry = (int)s_warpmax[w] > carry ? (int)s_warpmax[w] : carry;
-      int prev = __shfl_up_sync(0xffffffffu, wm, 1);
-      if (lane > 0) carry = prev > carry ? prev : carry;
-#pragma unroll
-      for (int r = 0; r < VT; ++r) s_own[threadIdx.x * VT + r] = loc[r] > carry ? loc[r] : carry;
     }
     __syncthreads();
     uint32_t bal[VT];
@@ -340,6 +369,7 @@ __global__ void __launch_bounds__(kNT) k_expand(GasArgs<P> a) {
       if (k < cnt) {
         const int j = s_own[k];
         const int el = k - s_base[j] - 1;
+        my_bytes += (el >= 0) ? (unsigned long long)(4 + probe_bytes_trait<P>::value) : 12ull;
         if (el >= 0) {
           const int v = s_v[j];
           const int eid = s_rs[j] + el;
@@ -370,6 +400,7 @@ __global__ void __launch_bounds__(kNT) k_expand(GasArgs<P> a) {
       }
       bal[r] = __ballot_sync(0xffffffffu, surv);
       outv[r] = fo;
+      if (surv) my_bytes += 8;  // queue entry + the Program's per-vertex write
       if (lane == 0) s_cnt[r * kNW + warp] = __popc(bal[r]);
     }
     __syncthreads();
@@ -416,6 +447,7 @@ __global__ void __launch_bounds__(kNT) k_expand(GasArgs<P> a) {
       }
     }
   }
+  add_bytes(ctl->kbytes, KID_EXPAND, my_bytes);
   if (track_next_edges_trait<P>::value) {
     my_edges = warp_sum(my_edges);
     if (lane == 0 && my_edges) atomicAdd(&s_edges, my_edges);

@@ -68,12 +68,12 @@ int run_gas(mg_graph *g, const GasArgs<P> &a, uint32_t n0, const mg_options *o, 
   const int post_all = P::postApplyOverEdges() == POST_APPLY_ALL;
   const int kpl = 3 + (gather ? 1 : 0) + (apply ? 1 : 0) + (post ? 1 : 0);
   LevelBody body = [=](cudaStream_t ss, cudaGraphConditionalHandle h, int use_h) {
-    if (gather) k_gather<P><<<grid, kNT, 0, ss>>>(a);
-    if (apply) k_apply<P><<<grid, kNT, 0, ss>>>(a, apply_all, gather ? 1 : 0);
-    if (post) k_post_apply<P><<<grid, kNT, 0, ss>>>(a, post_all);
-    k_frontier_scan<P, kVTS, kVT><<<grid, kNT, 0, ss>>>(a);
-    k_expand<P, kVT><<<grid, kNT, 0, ss>>>(a);
-    k_level_end<<<1, 32, 0, ss>>>(a.ctl, h, use_h);
+    if (gather) MG_LAUNCH(KID_GATHER, ss, k_gather<P><<<grid, kNT, 0, ss>>>(a));
+    if (apply) MG_LAUNCH(KID_APPLY, ss, k_apply<P><<<grid, kNT, 0, ss>>>(a, apply_all, gather ? 1 : 0));
+    if (post) MG_LAUNCH(KID_APPLY, ss, k_post_apply<P><<<grid, kNT, 0, ss>>>(a, post_all));
+    MG_LAUNCH(KID_SCAN, ss, (k_frontier_scan<P, kVTS, kVT><<<grid, kNT, 0, ss>>>(a)));
+    MG_LAUNCH(KID_EXPAND, ss, (k_expand<P, kVT><<<grid, kNT, 0, ss>>>(a)));
+    MG_LAUNCH(KID_OTHER, ss, k_level_end<<<1, 32, 0, ss>>>(a.ctl, h, use_h));
   };
   st = run_level_loop(g, s, std::string(name) + "/" + std::to_string(grid), kpl, body, o->use_cuda_graph != 0, res);
   if (st != MG_OK) return st;
@@ -88,7 +88,7 @@ static void fill_stats(mg_stats *stats, const LoopResult &res) {
   stats->iterations = (int32_t)res.ctl.level;
   stats->push_iterations = (int32_t)res.ctl.level;
   stats->pull_iterations = 0;
-  stats->converged = res.ctl.active ? 0 : 1;
+  stats->converged = (res.ctl.frontier_size == 0) ? 1 : 0;
   stats->device_ms = res.ms;
   stats->vertices_reached = 0;
   stats->edges_traversed = 0;

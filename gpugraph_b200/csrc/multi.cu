@@ -1,0 +1,671 @@
+// Batched traversal: up to 64 BFS or SSSP sources in one pass, carried as a
+// 64-bit mask per vertex (north_star "batching"). The reference runs sources
+// one after the other (Algorithms/BFS/bfs.cu:865-881, Algorithms/SSSP/sssp.cu:389-404);
+// here one sweep over an edge serves every source whose frontier contains its
+// tail, so the column indices are read once per level instead of once per
+// source and level.
+//
+// HBM layout (per graph, allocated on first use):
+//   mask[0]      visit[V]   u64: bit s set once source s has reached v (BFS)
+//   mask[1..2]   F[2][V]    u64: level-parity frontier masks
+//   multi_out    [V][64]    int32 per-source results (256 contiguous bytes per vertex)
+// Results are transposed to the caller's [nsrc][V] layout at the end.
+//
+// BFS levels switch between push (the GAS engine's load-balanced expand with
+// an OR-into-mask Program, next frontier as a vertex queue) and pull (every
+// vertex still missing sources ORs its in-neighbours' frontier masks, stopping
+// as soon as every missing source is found). SSSP relaxes warp-per-edge:
+// lane l owns sources l and l+32, so one edge reads the two 256-byte distance
+// rows with coalesced loads and atomicMin's only improved entries.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <vector>
+
+#include "algo_util.cuh"
+#include "gas/driver.cuh"
+#include "gas/engine.cuh"
+#include "gas/programs.cuh"
+
+namespace mg {
+
+typedef unsigned long long u64;
+constexpr int kMVTS = 4;
+constexpr int kMVT = 8;
+
+// Push step of the batched BFS as a GAS Program: expand_edge emits the
+// sources that reach the neighbour for the first time, contract ORs them into
+// the neighbour's next-level mask; the engine's bitmap puts each neighbour in
+// the next queue once.
+struct msbfs_push {
+  typedef int DataType;
+  typedef u64 MiscType;
+  typedef int GatherType;
+  typedef int VertexId;
+  typedef int SizeT;
+  static const int INIT_VALUE = -1;
+  static const bool allow_duplicates = false;
+  static const bool track_next_edges = true;
+  static const int probe_bytes = 8;  // the neighbour's visit mask
+  struct VertexType {
+    u64 *visit;
+    u64 *F0;
+    u64 *F1;
+  };
+  struct EdgeType {
+    int nodes;
+  };
+  static SrcVertex srcVertex() { return SINGLE; }
+  static GatherEdges gatherOverEdges() { return NO_GATHER_EDGES; }
+  static ApplyVertices applyOverEdges() { return NO_APPLY_VERTICES; }
+  static PostApplyVertices postApplyOverEdges() { return NO_POST_APPLY_VERTICES; }
+  static ExpandEdges expandOverEdges() { return EXPAND_OUT_EDGES; }
+  struct expand_vertex {
+    __device__ bool operator()(const int, const char, VertexType &, EdgeType &) { return true; }
+  };
+  struct expand_edge {
+    __device__ void operator()(const bool, const int iteration, const int u, const int v, const int, VertexType &vl,
+                               EdgeType &, int &frontier, u64 &misc) {
+      const u64 f = (iteration & 1) ? vl.F1[u] : vl.F0[u];
+      const u64 m = f & ~vl.visit[v];
+      if (m) {
+        frontier = v;
+        misc = m;
+      }
+    }
+  };
+  struct contract {
+    __device__ void operator()(const int iteration, int &v, VertexType &vl, EdgeType &, int *, u64 &misc) {
+      u64 *nx = (iteration & 1) ? vl.F0 : vl.F1;
+      if ((nx[v] | misc) != nx[v]) atomicOr(&nx[v], misc);
+    }
+  };
+};
+
+struct MultiArgs {
+  DevCsr g;
+  u64 *visit, *F0, *F1;
+  int32_t *out;  // [V][64]
+  int32_t *q0, *q1;
+  uint32_t *bm0, *bm1;
+  unsigned long long *status;
+  Ctl *ctl;
+  u64 all;  // mask of the sources in use
+};
+
+MG_DEVINL u64 *cur_F(const MultiArgs &a, uint32_t L) { return (L & 1) ? a.F1 : a.F0; }
+MG_DEVINL u64 *nxt_F(const MultiArgs &a, uint32_t L) { return (L & 1) ? a.F0 : a.F1; }
+MG_DEVINL int32_t *cur_Q(const MultiArgs &a, uint32_t L) { return (L & 1) ? a.q1 : a.q0; }
+MG_DEVINL int32_t *nxt_Q(const MultiArgs &a, uint32_t L) { return (L & 1) ? a.q0 : a.q1; }
+
+MG_DEVINL void write_bits(int32_t *row, u64 bits, int32_t value) {
+  while (bits) {
+    const int b = __ffsll((long long)bits) - 1;
+    bits &= bits - 1;
+    row[b] = value;
+  }
+}
+
+__global__ void k_ms_init(MultiArgs a, const int32_t *srcs, int32_t nsrc) {
+  for (int s = threadIdx.x; s < nsrc; s += blockDim.x) {
+    const int v = srcs[s];
+    atomicOr(&a.F0[v], 1ull << s);
+    atomicOr(&a.visit[v], 1ull << s);
+    a.out[(int64_t)v * 64 + s] = 0;
+  }
+}
+
+// Start of a level after a push level: the queued vertices keep only their
+// new sources (depth = level), and the previous level's masks are cleared.
+__global__ void __launch_bounds__(kNT) k_ms_apply(MultiArgs a) {
+  Ctl *ctl = a.ctl;
+  if (!ctl->active || !ctl->apply_pending) return;
+  const uint32_t L = ctl->level, n = ctl->frontier_size, pn = ctl->prev_size;
+  u64 *Fc = cur_F(a, L), *Fp = nxt_F(a, L);
+  const int32_t *Q = cur_Q(a, L), *Qp = nxt_Q(a, L);
+  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    const int v = Q[i];
+    const u64 vis = a.visit[v];
+    const u64 nb = Fc[v] & ~vis;
+    Fc[v] = nb;
+    if (nb) {
+      a.visit[v] = vis | nb;
+      write_bits(a.out + (int64_t)v * 64, nb, (int32_t)L);
+    }
+  }
+  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < pn; i += gridDim.x * blockDim.x) Fp[Qp[i]] = 0;
+}
+
+// Pull level: lane per vertex, warp per 32 consecutive vertices.
+__global__ void __launch_bounds__(kNT) k_ms_pull(MultiArgs a) {
+  __shared__ unsigned long long s_cnt, s_edges;
+  Ctl *ctl = a.ctl;
+  if (!ctl->active || ctl->mode != MODE_BITMAP) return;
+  const uint32_t L = ctl->level;
+  const u64 *Fc = cur_F(a, L);
+  u64 *Fn = nxt_F(a, L);
+  const int32_t V = a.g.V;
+  const int32_t *coff = a.g.csc_offsets, *crow = a.g.csc_rows, *ro = a.g.row_offsets;
+  if (threadIdx.x == 0) {
+    s_cnt = 0;
+    s_edges = 0;
+  }
+  __syncthreads();
+  unsigned long long my_cnt = 0, my_edges = 0, my_bytes = 0;
+  for (int64_t v = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; v < V; v += (int64_t)gridDim.x * blockDim.x) {
+    const u64 vis = a.visit[v];
+    const u64 need = a.all & ~vis;
+    u64 acc = 0;
+    my_bytes += 16;  // visit read + next-mask write
+    if (need) {
+      const int beg = coff[v], end = coff[v + 1];
+      int e = beg;
+      for (; e < end; ++e) {
+        acc |= __ldg(&Fc[crow[e]]);
+        if ((acc & need) == need) {
+          ++e;
+          break;
+        }
+      }
+      my_bytes += 8 + 12ull * (unsigned long long)(e - beg);  // offsets; row index + mask per edge
+      acc &= need;
+    }
+    Fn[v] = acc;
+    if (acc) {
+      my_bytes += 8 + 4ull * (unsigned long long)__popcll(acc);  // visit write + depths
+      a.visit[v] = vis | acc;
+      write_bits(a.out + v * 64, acc, (int32_t)L + 1);
+      my_cnt += 1;
+      my_edges += (unsigned long long)(ro[v + 1] - ro[v]);
+    }
+  }
+  add_bytes(ctl->kbytes, KID_MS_PULL, my_bytes);
+  my_cnt = warp_sum(my_cnt);
+  my_edges = warp_sum(my_edges);
+  if (lane_id() == 0 && (my_cnt || my_edges)) {
+    atomicAdd(&s_cnt, my_cnt);
+    atomicAdd(&s_edges, my_edges);
+  }
+  __syncthreads();
+  if (threadIdx.x == 0 && (s_cnt || s_edges)) {
+    atomicAdd((unsigned long long *)&ctl->acc[0], s_cnt);
+    atomicAdd(&ctl->next_edges, s_edges);
+  }
+}
+
+// Pull -> push: ordered compaction of the vertices with a non-empty mask into
+// the queue; clears the other parity's masks and both dedup bitmaps.
+__global__ void __launch_bounds__(kNT) k_ms_convert(MultiArgs a) {
+  constexpr int VPT = 4;
+  constexpr uint32_t TV = kNT * VPT;
+  __shared__ uint32_t s_red[kNW + 1];
+  __shared__ uint32_t s_tile, s_prefix;
+  __shared__ int s_fail;
+  Ctl *ctl = a.ctl;
+  if (!ctl->active || !ctl->convert) return;
+  const uint32_t L = ctl->level, epoch = ctl->epoch + 2;
+  const uint32_t V = (uint32_t)a.g.V;
+  const u64 *Fc = cur_F(a, L);
+  u64 *Fo = nxt_F(a, L);
+  int32_t *Q = cur_Q(a, L);
+  const uint32_t words = (V + 31) / 32;
+  for (uint32_t w = blockIdx.x * blockDim.x + threadIdx.x; w < words; w += gridDim.x * blockDim.x) {
+    a.bm0[w] = 0;
+    a.bm1[w] = 0;
+  }
+  const uint32_t ntiles = (V + TV - 1) / TV;
+  if (threadIdx.x == 0) s_fail = 0;
+  for (;;) {
+    const uint32_t tile = next_tile(&ctl->tile_ctr[3], &s_tile);
+    if (tile >= ntiles || s_fail) break;
+    const uint32_t vb = tile * TV + threadIdx.x * VPT;
+    uint32_t flags = 0, c = 0;
+#pragma unroll
+    for (int k = 0; k < VPT; ++k) {
+      if (vb + k < V) {
+        if (Fc[vb + k]) {
+          flags |= 1u << k;
+          ++c;
+        }
+        Fo[vb + k] = 0;
+      }
+    }
+    uint32_t tot;
+    const uint32_t ex = cta_exclusive_sum(c, s_red, &tot);
+    if (warp_id() == 0) {
+      bool failed = false;
+      const uint32_t pre = lookback(a.status, tile, tot, epoch, ctl->spin_limit, &failed);
+      if (lane_id() == 0) {
+        s_prefix = pre;
+        if (failed) {
+          s_fail = 1;
+          raise_error(ctl, MG_ERR_TIMEOUT);
+        } else if (tile == ntiles - 1) {
+          ctl->frontier_size = pre + tot;
+        }
+      }
+    }
+    __syncthreads();
+    if (s_fail) break;
+    uint32_t pos = s_prefix + ex;
+#pragma unroll
+    for (int k = 0; k < VPT; ++k)
+      if ((flags >> k) & 1u) {
+        if (pos < V) Q[pos] = (int32_t)(vb + k);
+        ++pos;
+      }
+  }
+}
+
+__global__ void k_ms_level_end(Ctl *ctl, int32_t V, int64_t E, cudaGraphConditionalHandle h, int use_handle) {
+  if (threadIdx.x != 0) return;
+  if (ctl->active) {
+    const uint32_t mode = ctl->mode;
+    uint32_t n_next;
+    if (mode == MODE_BITMAP) {
+      unsigned long long *cnt = (unsigned long long *)&ctl->acc[0];
+      n_next = (uint32_t)*cnt;
+      *cnt = 0;
+      ctl->pull_levels += 1;
+    } else {
+      n_next = ctl->next_size;
+      ctl->push_levels += 1;
+    }
+    const unsigned long long m_next = ctl->next_edges;
+    uint32_t new_mode = mode;
+    if (ctl->dir_policy == MG_DIR_PUSH) {
+      new_mode = MODE_QUEUE;
+    } else if (ctl->dir_policy == MG_DIR_PULL) {
+      new_mode = MODE_BITMAP;
+    } else if (mode == MODE_QUEUE) {
+      if ((double)m_next > (double)E / (double)ctl->alpha) new_mode = MODE_BITMAP;
+    } else {
+      if ((double)n_next < (double)V / (double)ctl->beta && n_next < ctl->frontier_size) new_mode = MODE_QUEUE;
+    }
+    ctl->apply_pending = (mode == MODE_QUEUE) ? 1u : 0u;
+    ctl->convert = (mode == MODE_BITMAP && new_mode == MODE_QUEUE) ? 1u : 0u;
+    ctl->mode = new_mode;
+    ctl->prev_size = ctl->frontier_size;
+    ctl->level += 1;
+    ctl->frontier_size = n_next;
+    ctl->next_size = 0;
+    ctl->edge_total = 0;
+    ctl->exp_tiles = 0;
+    ctl->next_edges = 0;
+    ctl->epoch += 4;
+    for (int i = 0; i < 4; ++i) ctl->tile_ctr[i] = 0;
+    ctl->active = (n_next > 0 && ctl->level < ctl->max_iter && ctl->error == 0) ? 1u : 0u;
+  }
+  if (use_handle) cudaGraphSetConditional(h, ctl->active);
+}
+
+// [V][64] -> [ns][V] for sources s_begin .. s_begin+ns-1, 32 vertices per tile
+// through shared memory (coalesced on both sides).
+__global__ void k_ms_transpose(const int32_t *in, int32_t *out, int32_t V, int32_t s_begin, int32_t ns) {
+  __shared__ int32_t t[32][65];
+  const int64_t v0 = (int64_t)blockIdx.x * 32;
+  for (int i = threadIdx.x; i < 32 * 64; i += blockDim.x) {
+    const int r = i / 64, c = i % 64;
+    t[r][c] = (v0 + r < V) ? in[(v0 + r) * 64 + c] : 0;
+  }
+  __syncthreads();
+  for (int i = threadIdx.x; i < 32 * ns; i += blockDim.x) {
+    const int s = i / 32, r = i % 32;
+    if (v0 + r < V) out[(int64_t)s * V + v0 + r] = t[r][s_begin + s];
+  }
+}
+
+// ------------------------------------------------------------ batched SSSP --
+struct mssp_scan {
+  typedef int DataType;
+  typedef int MiscType;
+  typedef int GatherType;
+  typedef int VertexId;
+  typedef int SizeT;
+  struct VertexType {
+    int nodes;
+  };
+  struct EdgeType {
+    int nodes;
+  };
+  struct expand_vertex {
+    __device__ bool operator()(const int, const char, VertexType &, EdgeType &) { return true; }
+  };
+};
+
+// Clears the previous level's masks (they were read by the previous expand).
+__global__ void __launch_bounds__(kNT) k_mss_clear(MultiArgs a) {
+  Ctl *ctl = a.ctl;
+  if (!ctl->active) return;
+  const uint32_t L = ctl->level, pn = ctl->prev_size;
+  u64 *Fp = nxt_F(a, L);
+  const int32_t *Qp = nxt_Q(a, L);
+  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < pn; i += gridDim.x * blockDim.x) Fp[Qp[i]] = 0;
+}
+
+template <int VT>
+__global__ void __launch_bounds__(kNT) k_mss_expand(MultiArgs a, const uint32_t *scan, const int32_t *part) {
+  constexpr int NV = kNT * VT;
+  constexpr int PER_WARP = NV / kNW;
+  __shared__ int32_t s_v[NV + 1];
+  __shared__ int32_t s_base[NV + 1];
+  __shared__ int32_t s_rs[NV + 1];
+  __shared__ int32_t s_own[NV];
+  __shared__ uint32_t s_tile, s_warpmax[kNW];
+  __shared__ int s_fail;
+  Ctl *ctl = a.ctl;
+  if (!ctl->active) return;
+  const uint32_t L = ctl->level, n = ctl->frontier_size, total = ctl->edge_total, ntiles = ctl->exp_tiles;
+  const unsigned long long items = (unsigned long long)n + total;
+  const int32_t *Q = cur_Q(a, L);
+  int32_t *Qn = nxt_Q(a, L);
+  const u64 *Fc = cur_F(a, L);
+  u64 *Fn = nxt_F(a, L);
+  uint32_t *dedup = (L & 1) ? a.bm0 : a.bm1;
+  const int32_t *ro = a.g.row_offsets, *col = a.g.col, *wgt = a.g.wgt;
+  const int32_t V = a.g.V;
+  const int lane = lane_id(), warp = warp_id();
+  unsigned long long my_bytes = 0;
+  if (threadIdx.x == 0) s_fail = 0;
+  for (;;) {
+    const uint32_t tile = next_tile(&ctl->tile_ctr[1], &s_tile);
+    if (tile >= ntiles || s_fail) break;
+    int cnt;
+    if (!decode_tile<VT>(tile, ntiles, n, items, part, scan, Q, ro, s_v, s_base, s_rs, s_own, s_warpmax, &cnt,
+                         [](int, int) {})) {
+      if (threadIdx.x == 0) {
+        raise_error(ctl, MG_ERR_OVERFLOW);
+        s_fail = 1;
+      }
+      __syncthreads();
+      break;
+    }
+    const int k0 = warp * PER_WARP;
+    const int k1 = min(cnt, k0 + PER_WARP);
+    for (int k = k0; k < k1; ++k) {
+      const int j = s_own[k];
+      const int el = k - s_base[j] - 1;
+      if (el < 0) continue;
+      const int u = s_v[j];
+      const int eid = s_rs[j] + el;
+      if ((unsigned)eid >= (unsigned)a.g.E) {
+        raise_error(ctl, MG_ERR_OVERFLOW);
+        continue;
+      }
+      const int v = col[eid];
+      const int w = wgt[eid];
+      const u64 am = Fc[u];
+      // column, weight, source mask; both distances of every active source
+      if (lane == 0) my_bytes += 16 + 8ull * (unsigned long long)__popcll(am);
+      const bool b0 = (am >> lane) & 1ull, b1 = (am >> (lane + 32)) & 1ull;
+      bool imp0 = false, imp1 = false;
+      if (b0 | b1) {
+        const int32_t *du = a.out + (int64_t)u * 64;
+        int32_t *dv = a.out + (int64_t)v * 64;
+        if (b0) {
+          const int c = du[lane] + w;
+          if (c < dv[lane]) imp0 = atomicMin(&dv[lane], c) > c;
+        }
+        if (b1) {
+          const int c = du[lane + 32] + w;
+          if (c < dv[lane + 32]) imp1 = atomicMin(&dv[lane + 32], c) > c;
+        }
+      }
+      const u64 mask = (u64)__ballot_sync(0xffffffffu, imp0) | ((u64)__ballot_sync(0xffffffffu, imp1) << 32);
+      if (mask && lane == 0) {
+        my_bytes += 8 + 4ull * (unsigned long long)__popcll(mask);
+        atomicOr(&Fn[v], mask);
+        const uint32_t bit = 1u << (v & 31);
+        if (!(ld_volatile(&dedup[v >> 5]) & bit) && !(atomicOr(&dedup[v >> 5], bit) & bit)) {
+          const uint32_t pos = atomicAdd(&ctl->next_size, 1u);
+          if (pos < (uint32_t)V) Qn[pos] = v;
+          else raise_error(ctl, MG_ERR_OVERFLOW);
+        }
+      }
+    }
+  }
+  add_bytes(ctl->kbytes, KID_MSS_EXPAND, my_bytes);
+}
+
+__global__ void k_mss_level_end(Ctl *ctl, cudaGraphConditionalHandle h, int use_handle) {
+  if (threadIdx.x != 0) return;
+  if (ctl->active) {
+    ctl->prev_size = ctl->frontier_size;
+    ctl->level += 1;
+    ctl->push_levels += 1;
+    ctl->frontier_size = ctl->next_size;
+    ctl->next_size = 0;
+    ctl->edge_total = 0;
+    ctl->exp_tiles = 0;
+    ctl->epoch += 4;
+    for (int i = 0; i < 4; ++i) ctl->tile_ctr[i] = 0;
+    ctl->active = (ctl->frontier_size > 0 && ctl->level < ctl->max_iter && ctl->error == 0) ? 1u : 0u;
+  }
+  if (use_handle) cudaGraphSetConditional(h, ctl->active);
+}
+
+__global__ void k_mss_init(MultiArgs a, const int32_t *srcs, int32_t nsrc) {
+  for (int s = threadIdx.x; s < nsrc; s += blockDim.x) {
+    const int v = srcs[s];
+    atomicOr(&a.F0[v], 1ull << s);
+    a.out[(int64_t)v * 64 + s] = 0;
+  }
+}
+
+static MultiArgs multi_args(mg_graph *g) {
+  MultiArgs a;
+  a.g = g->csr;
+  a.visit = g->mask[0];
+  a.F0 = g->mask[1];
+  a.F1 = g->mask[2];
+  a.out = g->multi_out;
+  a.q0 = g->ws.queue[0];
+  a.q1 = g->ws.queue[1];
+  a.bm0 = g->ws.bm[0];
+  a.bm1 = g->ws.bm[1];
+  a.status = g->ws.status;
+  a.ctl = g->ws.ctl;
+  a.all = 0;
+  return a;
+}
+
+static int multi_prepare(mg_graph *g, const int32_t *srcs, int32_t nsrc, const mg_options *o, cudaStream_t s,
+                         std::vector<int32_t> *distinct, int32_t fill) {
+  if (nsrc < 1 || nsrc > 64) return set_error(MG_ERR_ARG, "nsrc must be in [1, 64]");
+  int st = check_sources(g, srcs, nsrc, distinct);
+  if (st != MG_OK) return st;
+  if ((st = ensure_workspace(g)) != MG_OK) return st;
+  if ((st = ensure_multi(g, true)) != MG_OK) return st;
+  if ((st = prepare_run(g, s)) != MG_OK) return st;
+  const size_t V = (size_t)g->nodes;
+  cudaError_t e = cudaMemsetAsync(g->mask[0], 0, V * 8, s);
+  if (e == cudaSuccess) e = cudaMemsetAsync(g->mask[1], 0, V * 8, s);
+  if (e == cudaSuccess) e = cudaMemsetAsync(g->mask[2], 0, V * 8, s);
+  if (e == cudaSuccess) e = cudaMemsetAsync(g->ws.bm[0], 0, g->ws.words * 4, s);
+  if (e == cudaSuccess) e = cudaMemsetAsync(g->ws.bm[1], 0, g->ws.words * 4, s);
+  if (e == cudaSuccess && fill == -1) e = cudaMemsetAsync(g->multi_out, 0xff, V * 64 * 4, s);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(g->ws.queue[0], distinct->data(), distinct->size() * 4, cudaMemcpyHostToDevice, s);
+  // the per-source source list goes in scan[] (free until the first scan)
+  if (e == cudaSuccess) e = cudaMemcpyAsync(g->ws.scan, srcs, (size_t)nsrc * 4, cudaMemcpyHostToDevice, s);
+  if ((st = cuda_status(e, "batched init")) != MG_OK) return st;
+  if (fill != -1) {
+    k_fill_i32<<<g->num_sms * 8, 256, 0, s>>>(g->multi_out, fill, (int64_t)V * 64);
+    count_launch();
+  }
+  (void)o;
+  return MG_OK;
+}
+
+static int multi_finish(mg_graph *g, cudaStream_t s, int32_t nsrc, int32_t *out, int32_t unreached, mg_stats *stats,
+                        const mg_options *o, const LoopResult &res) {
+  finish_run(g, res.ctl.level);
+  if (res.ctl.error) return set_error(res.ctl.error, std::string("batched traversal: device reported ") +
+                                                         mg_status_string(res.ctl.error));
+  int st;
+  if (stats) {
+    stats->iterations = (int32_t)res.ctl.level;
+    stats->push_iterations = (int32_t)res.ctl.push_levels;
+    stats->pull_iterations = (int32_t)res.ctl.pull_levels;
+    stats->converged = res.ctl.frontier_size == 0 ? 1 : 0;
+    stats->device_ms = res.ms;
+    stats->vertices_reached = 0;
+    stats->edges_traversed = 0;
+    if (want_stats(o) &&
+        (st = reach_stats(g, s, g->multi_out, unreached, nsrc, 64, &stats->vertices_reached, &stats->edges_traversed)) !=
+            MG_OK)
+      return st;
+  }
+  const int32_t V = g->csr.V;
+  const unsigned nblk = (unsigned)((V + 31) / 32);
+  if (o->outputs_on_device) {
+    k_ms_transpose<<<nblk, 256, 0, s>>>(g->multi_out, out, V, 0, nsrc);
+    count_launch();
+    return cuda_status(cudaStreamSynchronize(s), "batched result transpose");
+  }
+  // Host output: transpose two sources at a time into the (now free) V x 8-byte
+  // mask buffers, rotating over the three so transposes overlap the copies.
+  for (int s0 = 0, c = 0; s0 < nsrc; s0 += 2, ++c) {
+    const int ns = std::min(2, nsrc - s0);
+    int32_t *buf = reinterpret_cast<int32_t *>(g->mask[c % 3]);
+    k_ms_transpose<<<nblk, 256, 0, s>>>(g->multi_out, buf, V, s0, ns);
+    count_launch();
+    cudaError_t e = cudaMemcpyAsync(out + (int64_t)s0 * V, buf, (size_t)ns * V * 4, cudaMemcpyDeviceToHost, s);
+    if (e != cudaSuccess) return cuda_status(e, "batched result copy");
+  }
+  return cuda_status(cudaStreamSynchronize(s), "batched result copy");
+}
+
+}  // namespace mg
+
+using namespace mg;
+
+static const mg_options *opts_or_default(const mg_options *o, mg_options *d) {
+  if (o) return o;
+  mg_options_init(d);
+  return d;
+}
+
+extern "C" {
+
+int mg_bfs_multi(mg_graph *g, const int32_t *srcs, int32_t nsrc, int32_t *depths, mg_stats *stats,
+                 const mg_options *opts) {
+  clear_error();
+  if (!g) return set_error(MG_ERR_ARG, "graph is NULL");
+  if (!depths) return set_error(MG_ERR_ARG, "depths is NULL");
+  mg_options d;
+  const mg_options *o = opts_or_default(opts, &d);
+  cudaStream_t s = run_stream(g, o);
+  std::vector<int32_t> distinct;
+  int st = multi_prepare(g, srcs, nsrc, o, s, &distinct, -1);
+  if (st != MG_OK) return st;
+  MultiArgs a = multi_args(g);
+  a.all = (nsrc == 64) ? ~0ull : ((1ull << nsrc) - 1);
+  GasArgs<msbfs_push> ga;
+  ga.g = g->csr;
+  ga.vl.visit = a.visit;
+  ga.vl.F0 = a.F0;
+  ga.vl.F1 = a.F1;
+  ga.el.nodes = (int)g->nodes;
+  ga.queue0 = g->ws.queue[0];
+  ga.queue1 = g->ws.queue[1];
+  ga.scan = g->ws.scan;
+  ga.part = g->ws.part;
+  ga.status = g->ws.status;
+  ga.bm0 = g->ws.bm[0];
+  ga.bm1 = g->ws.bm[1];
+  ga.changed = g->ws.changed;
+  ga.gather_tmp = g->ws.gather_tmp;
+  ga.gather_res = g->ws.gather_tmp;
+  ga.ctl = g->ws.ctl;
+  ga.expand_in = 0;
+  ga.gather_dir = NO_GATHER_EDGES;
+  const uint32_t max_iter = (uint32_t)std::min<int64_t>(o->iter_num > 0 ? o->iter_num : 0, g->nodes + 2);
+  const int dir = o->direction;
+  k_ctl_init<<<1, 32, 0, s>>>(g->ws.ctl, (uint32_t)distinct.size(), max_iter, (unsigned long long)o->spin_limit,
+                              dir == MG_DIR_PULL ? MODE_BITMAP : MODE_QUEUE);
+  k_ms_init<<<1, 64, 0, s>>>(a, reinterpret_cast<const int32_t *>(g->ws.scan), nsrc);
+  count_launch(2);
+  // direction policy and switch factors in the control block
+  Ctl init_fields;
+  (void)init_fields;
+  struct {
+    uint32_t dir;
+    float alpha, beta;
+  } pol = {(uint32_t)dir, (float)o->alpha, (float)o->beta};
+  cudaError_t e = cudaMemcpyAsync(&g->ws.ctl->dir_policy, &pol.dir, 4, cudaMemcpyHostToDevice, s);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(&g->ws.ctl->alpha, &pol.alpha, 4, cudaMemcpyHostToDevice, s);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(&g->ws.ctl->beta, &pol.beta, 4, cudaMemcpyHostToDevice, s);
+  if ((st = cuda_status(e, "batched bfs policy")) != MG_OK) return st;
+  if (dir == MG_DIR_PULL) {
+    // The pull sweep reads the dense level-0 masks (already in F0).
+  }
+  const int grid = persistent_grid(g, o, 4);
+  const int32_t V = g->csr.V;
+  const int64_t E = g->edges;
+  LevelBody body = [=](cudaStream_t ss, cudaGraphConditionalHandle h, int use_h) {
+    MG_LAUNCH(KID_MS_APPLY, ss, k_ms_apply<<<grid, kNT, 0, ss>>>(a));
+    MG_LAUNCH(KID_CONVERT, ss, k_ms_convert<<<grid, kNT, 0, ss>>>(a));
+    MG_LAUNCH(KID_SCAN, ss, (k_frontier_scan<msbfs_push, kMVTS, kMVT><<<grid, kNT, 0, ss>>>(ga)));
+    MG_LAUNCH(KID_EXPAND, ss, (k_expand<msbfs_push, kMVT><<<grid, kNT, 0, ss>>>(ga)));
+    MG_LAUNCH(KID_MS_PULL, ss, k_ms_pull<<<grid, kNT, 0, ss>>>(a));
+    MG_LAUNCH(KID_OTHER, ss, k_ms_level_end<<<1, 32, 0, ss>>>(a.ctl, V, E, h, use_h));
+  };
+  LoopResult res;
+  st = run_level_loop(g, s, "bfs_multi/" + std::to_string(grid), 6, body, o->use_cuda_graph != 0, &res);
+  if (st != MG_OK) return st;
+  if (res.ctl.apply_pending && res.ctl.frontier_size == 0) {
+    // nothing left to apply: the last push level produced an empty queue
+  }
+  return multi_finish(g, s, nsrc, depths, -1, stats, o, res);
+}
+
+int mg_sssp_multi(mg_graph *g, const int32_t *srcs, int32_t nsrc, int32_t *dists, mg_stats *stats,
+                  const mg_options *opts) {
+  clear_error();
+  if (!g) return set_error(MG_ERR_ARG, "graph is NULL");
+  if (!dists) return set_error(MG_ERR_ARG, "dists is NULL");
+  if (!g->csr.wgt) return set_error(MG_ERR_UNSUPPORTED, "SSSP needs int32 edge weights (value_type MG_VAL_I32)");
+  mg_options d;
+  const mg_options *o = opts_or_default(opts, &d);
+  cudaStream_t s = run_stream(g, o);
+  std::vector<int32_t> distinct;
+  int st = multi_prepare(g, srcs, nsrc, o, s, &distinct, programs::sssp::INIT_VALUE);
+  if (st != MG_OK) return st;
+  MultiArgs a = multi_args(g);
+  a.all = (nsrc == 64) ? ~0ull : ((1ull << nsrc) - 1);
+  GasArgs<mssp_scan> ga;
+  ga.g = g->csr;
+  ga.queue0 = g->ws.queue[0];
+  ga.queue1 = g->ws.queue[1];
+  ga.scan = g->ws.scan + 0;
+  ga.part = g->ws.part;
+  ga.status = g->ws.status;
+  ga.bm0 = g->ws.bm[0];
+  ga.bm1 = g->ws.bm[1];
+  ga.changed = g->ws.changed;
+  ga.gather_tmp = g->ws.gather_tmp;
+  ga.gather_res = g->ws.gather_tmp;
+  ga.ctl = g->ws.ctl;
+  ga.expand_in = 0;
+  ga.gather_dir = NO_GATHER_EDGES;
+  const uint32_t max_iter = (uint32_t)std::min<int64_t>(o->iter_num > 0 ? o->iter_num : 0, g->nodes + 2);
+  k_ctl_init<<<1, 32, 0, s>>>(g->ws.ctl, (uint32_t)distinct.size(), max_iter, (unsigned long long)o->spin_limit,
+                              MODE_QUEUE);
+  k_mss_init<<<1, 64, 0, s>>>(a, reinterpret_cast<const int32_t *>(g->ws.scan), nsrc);
+  count_launch(2);
+  const int grid = persistent_grid(g, o, 4);
+  uint32_t *scan = g->ws.scan;
+  int32_t *part = g->ws.part;
+  LevelBody body = [=](cudaStream_t ss, cudaGraphConditionalHandle h, int use_h) {
+    MG_LAUNCH(KID_MS_APPLY, ss, k_mss_clear<<<grid, kNT, 0, ss>>>(a));
+    MG_LAUNCH(KID_SCAN, ss, (k_frontier_scan<mssp_scan, kMVTS, kMVT><<<grid, kNT, 0, ss>>>(ga)));
+    MG_LAUNCH(KID_MSS_EXPAND, ss, k_mss_expand<kMVT><<<grid, kNT, 0, ss>>>(a, scan, part));
+    MG_LAUNCH(KID_OTHER, ss, k_mss_level_end<<<1, 32, 0, ss>>>(a.ctl, h, use_h));
+  };
+  LoopResult res;
+  st = run_level_loop(g, s, "sssp_multi/" + std::to_string(grid), 4, body, o->use_cuda_graph != 0, &res);
+  if (st != MG_OK) return st;
+  return multi_finish(g, s, nsrc, dists, programs::sssp::INIT_VALUE, stats, o, res);
+}
+
+}  // extern "C"

@@ -4,12 +4,6 @@
 
 extern "C" {
 
-int mg_bfs_multi(mg_graph *, const int32_t *, int32_t, int32_t *, mg_stats *, const mg_options *) {
-  return mg::set_error(MG_ERR_UNSUPPORTED, "mg_bfs_multi not built");
-}
-int mg_sssp_multi(mg_graph *, const int32_t *, int32_t, int32_t *, mg_stats *, const mg_options *) {
-  return mg::set_error(MG_ERR_UNSUPPORTED, "mg_sssp_multi not built");
-}
 int mg_pagerank(mg_graph *, float *, mg_stats *, const mg_options *) {
   return mg::set_error(MG_ERR_UNSUPPORTED, "mg_pagerank not built");
 }

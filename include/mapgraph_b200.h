@@ -101,6 +101,14 @@ const char *mg_status_string(int status);
 int mg_abi_version(void);
 /* Number of device-side kernel launches issued by this thread since the last reset. */
 int64_t mg_kernel_launches(int reset);
+/* Per-kernel profiling for this thread (no reference counterpart; the reference
+ * has per-CTA clock() statistics, b40c/util/kernel_runtime_stats.cuh:55-86).
+ * While enabled, level loops run host-driven and every kernel launch is
+ * bracketed by CUDA events; enabling resets the accumulators. */
+int mg_profile_enable(int enable);
+/* Accumulated time, launch count and algorithmic bytes of kernel kind `kind`
+ * (0 <= kind < 12); *name receives a static string. */
+int mg_profile_read(int32_t kind, const char **name, double *total_ms, int64_t *launches, uint64_t *bytes);
 
 /* ----------------------------------------------------------------- graphs -- */
 /* Copy a host CSR to the device and build what the hot path needs (out-degrees,

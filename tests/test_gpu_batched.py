@@ -1,0 +1,112 @@
+"""GPU parity of the batched traversals: the 64-bit mask-frontier BFS/SSSP must
+equal independent per-source runs bit for bit, and the multi-graph batch must
+equal one BFS per graph."""
+import numpy as np
+import pytest
+
+import oracle
+from gpugraph_b200 import SSSP_INF, Graph, HostGraph, MapGraphError, _lib, concat_graphs
+
+pytestmark = pytest.mark.gpu
+
+DIRS = [_lib.MG_DIR_AUTO, _lib.MG_DIR_PUSH, _lib.MG_DIR_PULL]
+
+
+def seeded_sources(hg, n, seed=1):
+    rng = np.random.default_rng(seed)
+    cand = np.flatnonzero(np.diff(hg.row_offsets) > 0)
+    return rng.choice(cand, size=n, replace=False).astype(np.int32)
+
+
+@pytest.mark.parametrize("scale,ef,nsrc", [(14, 16, 64), (12, 8, 17), (10, 4, 1)])
+def test_bfs_multi_rmat(scale, ef, nsrc):
+    hg = HostGraph.rmat(scale, ef, seed=scale)
+    g = Graph(hg)
+    srcs = seeded_sources(hg, nsrc)
+    ref = np.stack([oracle.bfs(hg.row_offsets, hg.column_indices, s) for s in srcs])
+    for d in DIRS:
+        out, st = g.bfs_multi(srcs, direction=d)
+        assert np.array_equal(out, ref), d
+        reached = ref >= 0
+        deg = hg.out_degree()
+        assert st["vertices_reached"] == int(reached.sum())
+        assert st["edges_traversed"] == int((reached * deg[None, :]).sum())
+
+
+def test_bfs_multi_road_grid_and_duplicate_sources():
+    hg = HostGraph.road_grid(150, 0.02, 0.005, seed=5)
+    g = Graph(hg)
+    srcs = np.array([0, 11249, 22499, 0, 500] + list(range(1000, 1059)), np.int32)  # 64, with a duplicate
+    out, st = g.bfs_multi(srcs)
+    ref = np.stack([oracle.bfs(hg.row_offsets, hg.column_indices, s) for s in srcs])
+    assert np.array_equal(out, ref)
+    assert st["iterations"] > 100
+
+
+def test_bfs_multi_directed():
+    hg = HostGraph.rmat(12, 8, seed=21, symmetrize=False)
+    g = Graph(hg, directed=True)
+    srcs = seeded_sources(hg, 40, seed=3)
+    ref = np.stack([oracle.bfs(hg.row_offsets, hg.column_indices, s) for s in srcs])
+    for d in DIRS:
+        assert np.array_equal(g.bfs_multi(srcs, direction=d)[0], ref), d
+
+
+def test_bfs_multi_host_loop_equals_graph_loop():
+    hg = HostGraph.rmat(13, 16, seed=2)
+    g = Graph(hg)
+    srcs = seeded_sources(hg, 64)
+    a, _ = g.bfs_multi(srcs, use_cuda_graph=1)
+    b, _ = g.bfs_multi(srcs, use_cuda_graph=0)
+    assert np.array_equal(a, b)
+
+
+@pytest.mark.parametrize("scale,hi,nsrc", [(13, 64, 64), (11, 1000, 9)])
+def test_sssp_multi_rmat(scale, hi, nsrc):
+    hg = HostGraph.rmat(scale, 16, seed=scale).with_weights(1, hi, seed=4)
+    g = Graph(hg)
+    srcs = seeded_sources(hg, nsrc, seed=2)
+    out, st = g.sssp_multi(srcs)
+    for k, s in enumerate(srcs):
+        assert np.array_equal(out[k], oracle.sssp(hg.row_offsets, hg.column_indices, hg.edge_values, s)), k
+    single, _ = g.sssp(int(srcs[0]))
+    assert np.array_equal(single, out[0])
+
+
+def test_sssp_multi_road_grid_unreachable():
+    hg = HostGraph.road_grid(120, 0.3, 0.0, seed=8).with_weights(1, 1000, seed=8)  # 30% dropped: islands
+    g = Graph(hg)
+    srcs = np.arange(0, 14400, 225, dtype=np.int32)[:64]
+    out, _ = g.sssp_multi(srcs)
+    for k in (0, 17, 63):
+        ref = oracle.sssp(hg.row_offsets, hg.column_indices, hg.edge_values, srcs[k])
+        assert np.array_equal(out[k], ref)
+    assert (out == SSSP_INF).any()
+
+
+def test_multi_argument_errors():
+    hg = HostGraph.rmat(8, 4, seed=1)
+    g = Graph(hg)
+    with pytest.raises(MapGraphError) as e:
+        g.bfs_multi(np.arange(65, dtype=np.int32))
+    assert e.value.status == _lib.MG_ERR_ARG
+    with pytest.raises(MapGraphError) as e:
+        g.bfs_multi(np.array([0, 1 << 20], np.int32))
+    assert e.value.status == _lib.MG_ERR_ARG
+    with pytest.raises(MapGraphError) as e:
+        g.sssp_multi(np.array([0], np.int32))
+    assert e.value.status == _lib.MG_ERR_UNSUPPORTED
+
+
+def test_graph_batch_bfs():
+    rng = np.random.default_rng(7)
+    graphs = [HostGraph.rmat(int(s), 8, seed=100 + i) for i, s in enumerate(rng.integers(6, 12, size=24))]
+    big = concat_graphs(graphs)
+    g = Graph(big)
+    local = np.array([h.max_degree_vertex() for h in graphs], np.int32)
+    out, st = g.bfs_batch(local)
+    for i, h in enumerate(graphs):
+        b, e = big.graph_offsets[i], big.graph_offsets[i + 1]
+        assert np.array_equal(out[b:e], oracle.bfs(h.row_offsets, h.column_indices, local[i])), i
+    with pytest.raises(MapGraphError):
+        g.bfs_batch(np.full(24, 1 << 20, np.int32))
