@@ -32,7 +32,10 @@ class Options(C.Structure):
         ("tile_items", C.c_int32),
         ("ctas_per_sm", C.c_int32),
         ("compute_stats", C.c_int32),
-        ("reserved", C.c_int32 * 7),
+        ("pad0", C.c_int32),
+        ("alpha_multi", C.c_double),
+        ("ordered_frontier", C.c_int32),
+        ("reserved", C.c_int32 * 3),
     ]
 
 

@@ -25,7 +25,6 @@ constexpr int kVT = 8;   // items per thread in the expand (NV = 2048)
 
 // Bottom-up level: warp per 32-vertex bitmap word, lane per vertex.
 __global__ void __launch_bounds__(kNT) k_bfs_pull(GasArgs<BfsP> a) {
-  __shared__ unsigned long long s_cnt, s_edges;
   Ctl *ctl = a.ctl;
   if (!ctl->active || ctl->mode != MODE_BITMAP) return;
   const uint32_t level = ctl->level;
@@ -36,24 +35,34 @@ __global__ void __launch_bounds__(kNT) k_bfs_pull(GasArgs<BfsP> a) {
   const uint32_t words = ((uint32_t)V + 31) / 32;
   const int32_t *coff = a.g.csc_offsets, *crow = a.g.csc_rows, *ro = a.g.row_offsets;
   const int lane = lane_id();
-  if (threadIdx.x == 0) {
-    s_cnt = 0;
-    s_edges = 0;
-  }
-  __syncthreads();
   unsigned long long my_cnt = 0, my_edges = 0, my_bytes = 0;
-  const uint32_t nwarps = gridDim.x * kNW;
-  for (uint32_t w = blockIdx.x * kNW + warp_id(); w < words; w += nwarps) {
+  for (;;) {
+    // 32-vertex words are handed out dynamically (one atomic per word)
+    uint32_t w = 0;
+    if (lane == 0) w = atomicAdd(&ctl->group_ctr, 1u);
+    w = __shfl_sync(0xffffffffu, w, 0);
+    if (w >= words) break;
     const uint32_t vis = visited[w];
     const int v = (int)(w * 32 + lane);
     bool found = false;
     if (v < V && !((vis >> lane) & 1u)) {
       const int beg = coff[v], end = coff[v + 1];
       int e = beg;
-      for (; e < end; ++e) {
-        const int u = crow[e];
-        if ((__ldg(&cur[u >> 5]) >> (u & 31)) & 1u) {
+      // four in-edges per step (independent loads in flight); stop at the
+      // first step that finds a parent
+      while (e < end) {
+        const int c = min(4, end - e);
+        const int u0 = crow[e];
+        const int u1 = c > 1 ? crow[e + 1] : u0;
+        const int u2 = c > 2 ? crow[e + 2] : u0;
+        const int u3 = c > 3 ? crow[e + 3] : u0;
+        const uint32_t hit = ((__ldg(&cur[u0 >> 5]) >> (u0 & 31)) | (__ldg(&cur[u1 >> 5]) >> (u1 & 31)) |
+                              (__ldg(&cur[u2 >> 5]) >> (u2 & 31)) | (__ldg(&cur[u3 >> 5]) >> (u3 & 31))) &
+                             1u;
+        e += c;
+        if (hit) {
           found = true;
+          e -= 1;  // byte count below adds the found edge back
           break;
         }
       }
@@ -74,16 +83,10 @@ __global__ void __launch_bounds__(kNT) k_bfs_pull(GasArgs<BfsP> a) {
     }
   }
   add_bytes(ctl->kbytes, KID_BFS_PULL, my_bytes);
+  // per-warp totals straight to the control block (no block barrier at the end)
   my_edges = warp_sum(my_edges);
-  if (lane == 0) {
-    if (my_cnt) atomicAdd(&s_cnt, my_cnt);
-    if (my_edges) atomicAdd(&s_edges, my_edges);
-  }
-  __syncthreads();
-  if (threadIdx.x == 0) {
-    if (s_cnt) atomicAdd((unsigned long long *)&ctl->acc[0], s_cnt);
-    if (s_edges) atomicAdd(&ctl->next_edges, s_edges);
-  }
+  if (lane == 0 && my_cnt) atomicAdd((unsigned long long *)&ctl->acc[0], my_cnt);
+  if (lane == 0 && my_edges) atomicAdd(&ctl->next_edges, my_edges);
 }
 
 // Pull -> push conversion at the start of a level: ordered compaction of the
@@ -176,6 +179,7 @@ __global__ void k_bfs_level_end(Ctl *ctl, int32_t V, int64_t E, cudaGraphConditi
       if ((double)n_next < (double)V / (double)ctl->beta && n_next < ctl->frontier_size) new_mode = MODE_QUEUE;
     }
     ctl->convert = (mode == MODE_BITMAP && new_mode == MODE_QUEUE) ? 1u : 0u;
+    ctl->group_ctr = 0;
     ctl->mode = new_mode;
     ctl->level += 1;
     ctl->frontier_size = n_next;
@@ -264,7 +268,7 @@ int bfs_run(mg_graph *g, const std::vector<int32_t> &roots, int32_t *depths, mg_
   if ((st = cuda_status(e, "bfs init")) != MG_OK) return st;
   const int grid = persistent_grid(g, o, 4);
   k_fill_i32<<<g->num_sms * 4, 256, 0, s>>>(w.vbuf[0], BfsP::INIT_VALUE, V);
-  k_ctl_init<<<1, 32, 0, s>>>(w.ctl, nsrc, max_iter, (unsigned long long)o->spin_limit, MODE_QUEUE);
+  k_ctl_init<<<1, 32, 0, s>>>(w.ctl, nsrc, max_iter, (unsigned long long)o->spin_limit, MODE_QUEUE, ctl_flags(o));
   k_bfs_init<<<1, 256, 0, s>>>(w.ctl, w.queue[0], (int32_t)nsrc, w.vbuf[0], w.visited, w.bm[0], g->csr.row_offsets,
                                (uint32_t)o->direction, (float)o->alpha, (float)o->beta);
   count_launch(3);

@@ -39,8 +39,14 @@ struct Ctl {
   uint32_t pull_levels;
   uint32_t dir_policy;      // MG_DIR_* (BFS)
   uint32_t convert;         // 1: rebuild the queue from the bitmap at level start
+  uint32_t ordered;         // 1: compact the next frontier in tile order (look-back)
+  uint32_t group_ctr;       // dynamic work counter of the pull kernels
   uint32_t prev_size;       // |F| of the previous level (batched traversals)
   uint32_t apply_pending;   // 1: the previous push level left bits to apply
+  // Batched BFS: OR of the frontier masks of level parity p (the sources that
+  // can still reach new vertices); accumulated while the level's masks are
+  // produced, cleared once consumed.
+  unsigned long long srcmask[2];
   float alpha, beta;        // direction-switch factors (BFS)
   unsigned long long next_edges;     // sum of degrees of the next frontier
   unsigned long long visited_edges;  // sum of degrees of visited vertices (BFS)

@@ -37,7 +37,7 @@ __global__ void k_sequence_i32(int32_t *p, int64_t n) {
 }
 
 __global__ void k_ctl_init(Ctl *ctl, uint32_t frontier_size, uint32_t max_iter, unsigned long long spin_limit,
-                           uint32_t mode) {
+                           uint32_t mode, uint32_t flags) {
   if (threadIdx.x != 0) return;
   // The epoch keeps growing across runs so stale look-back words never match;
   // the host zeroes the status words and the control block before the 30-bit
@@ -52,6 +52,7 @@ __global__ void k_ctl_init(Ctl *ctl, uint32_t frontier_size, uint32_t max_iter, 
   c.mode = mode;
   c.next_mode = mode;
   c.active = (frontier_size > 0 && max_iter > 0) ? 1u : 0u;
+  c.ordered = flags & 1u;
   *ctl = c;
 }
 

@@ -326,6 +326,7 @@ __global__ void __launch_bounds__(kNT) k_expand(GasArgs<P> a) {
   const uint32_t level = ctl->level, n = ctl->frontier_size, total = ctl->edge_total;
   const uint32_t ntiles = ctl->exp_tiles, epoch = ctl->epoch + 1;
   const unsigned long long spin_limit = ctl->spin_limit;
+  const bool ordered = ctl->ordered != 0;
   const unsigned long long items = (unsigned long long)n + total;
   const int32_t *F = cur_queue(a, level);
   int32_t *Fout = nxt_queue(a, level);
@@ -425,16 +426,22 @@ __global__ void __launch_bounds__(kNT) k_expand(GasArgs<P> a) {
         run += x[q];
       }
       const uint32_t tile_total = __shfl_sync(0xffffffffu, inc, 31);
-      bool failed = false;
-      const uint32_t pre = lookback(a.status, tile, tile_total, epoch, spin_limit, &failed);
-      if (lane == 0) {
-        s_prefix = pre;
-        if (failed) {
-          s_fail = 1;
-          raise_error(ctl, MG_ERR_TIMEOUT);
-        } else if (tile == ntiles - 1) {
-          ctl->next_size = pre + tile_total;
+      if (ordered) {
+        // Deterministic frontier order: decoupled look-back over tiles.
+        bool failed = false;
+        const uint32_t pre = lookback(a.status, tile, tile_total, epoch, spin_limit, &failed);
+        if (lane == 0) {
+          s_prefix = pre;
+          if (failed) {
+            s_fail = 1;
+            raise_error(ctl, MG_ERR_TIMEOUT);
+          } else if (tile == ntiles - 1) {
+            ctl->next_size = pre + tile_total;
+          }
         }
+      } else if (lane == 0) {
+        // One atomic reservation per tile: no tile waits for another.
+        s_prefix = tile_total ? atomicAdd(&ctl->next_size, tile_total) : 0u;
       }
     }
     __syncthreads();
@@ -464,7 +471,9 @@ __global__ void k_level_end(Ctl *ctl, cudaGraphConditionalHandle h, int use_hand
 // --------------------------------------------------------------- utilities --
 __global__ void k_fill_i32(int32_t *p, int32_t v, int64_t n);
 __global__ void k_sequence_i32(int32_t *p, int64_t n);
+// flags: bit 0 = ordered frontier compaction (mg_options.ordered_frontier)
 __global__ void k_ctl_init(Ctl *ctl, uint32_t frontier_size, uint32_t max_iter, unsigned long long spin_limit,
-                           uint32_t mode);
+                           uint32_t mode, uint32_t flags);
+inline uint32_t ctl_flags(const mg_options *o) { return (o && o->ordered_frontier) ? 1u : 0u; }
 
 }  // namespace mg

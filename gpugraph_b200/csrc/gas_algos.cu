@@ -59,7 +59,7 @@ int run_gas(mg_graph *g, const GasArgs<P> &a, uint32_t n0, const mg_options *o, 
   if (e == cudaSuccess) e = cudaMemsetAsync(g->ws.changed, 0, (size_t)g->nodes, s);
   int st = cuda_status(e, "gas init");
   if (st != MG_OK) return st;
-  k_ctl_init<<<1, 32, 0, s>>>(a.ctl, n0, max_iter, (unsigned long long)o->spin_limit, MODE_QUEUE);
+  k_ctl_init<<<1, 32, 0, s>>>(a.ctl, n0, max_iter, (unsigned long long)o->spin_limit, MODE_QUEUE, ctl_flags(o));
   count_launch();
   const bool gather = P::gatherOverEdges() != NO_GATHER_EDGES;
   const bool apply = P::applyOverEdges() != NO_APPLY_VERTICES;

@@ -58,7 +58,7 @@ int ensure_workspace(mg_graph *g) {
     return st;
   MG_ALLOC(w.queue[0], V * 4);
   MG_ALLOC(w.queue[1], V * 4);
-  MG_ALLOC(w.scan, (V + 1) * 4);
+  MG_ALLOC(w.scan, (V + 1 + 64) * 4);  // also stages up to 64 batched sources
   MG_ALLOC(w.part, w.part_cap * 4);
   MG_ALLOC(w.status, w.status_cap * 8);
   MG_ALLOC(w.bm[0], w.words * 4);

@@ -128,6 +128,7 @@ void mg_options_init(mg_options *o) {
   o->tile_items = 0;
   o->ctas_per_sm = 0;
   o->compute_stats = 1;
+  o->alpha_multi = 5.0;
 }
 
 }  // extern "C"

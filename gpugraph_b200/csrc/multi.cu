@@ -113,6 +113,10 @@ __global__ void k_ms_init(MultiArgs a, const int32_t *srcs, int32_t nsrc) {
     atomicOr(&a.visit[v], 1ull << s);
     a.out[(int64_t)v * 64 + s] = 0;
   }
+  if (threadIdx.x == 0) {
+    a.ctl->srcmask[0] = a.all;
+    a.ctl->srcmask[1] = 0;
+  }
 }
 
 // Start of a level after a push level: the queued vertices keep only their
@@ -123,74 +127,129 @@ __global__ void __launch_bounds__(kNT) k_ms_apply(MultiArgs a) {
   const uint32_t L = ctl->level, n = ctl->frontier_size, pn = ctl->prev_size;
   u64 *Fc = cur_F(a, L), *Fp = nxt_F(a, L);
   const int32_t *Q = cur_Q(a, L), *Qp = nxt_Q(a, L);
+  u64 act = 0;
+  unsigned long long my_bytes = 0;
   for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
     const int v = Q[i];
     const u64 vis = a.visit[v];
     const u64 nb = Fc[v] & ~vis;
     Fc[v] = nb;
+    act |= nb;
+    my_bytes += 28;  // queue entry, visit and mask read, mask write
     if (nb) {
       a.visit[v] = vis | nb;
       write_bits(a.out + (int64_t)v * 64, nb, (int32_t)L);
+      my_bytes += 8 + 4ull * (unsigned long long)__popcll(nb);
     }
   }
-  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < pn; i += gridDim.x * blockDim.x) Fp[Qp[i]] = 0;
+  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < pn; i += gridDim.x * blockDim.x) {
+    Fp[Qp[i]] = 0;
+    my_bytes += 12;
+  }
+  add_bytes(ctl->kbytes, KID_MS_APPLY, my_bytes);
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) act |= __shfl_xor_sync(0xffffffffu, act, o);
+  if (lane_id() == 0 && act) atomicOr(&ctl->srcmask[L & 1], act);
 }
 
-// Pull level: lane per vertex, warp per 32 consecutive vertices.
+// OR of a 64-bit value over the warp.
+MG_DEVINL u64 warp_or(u64 x) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) x |= __shfl_xor_sync(0xffffffffu, x, o);
+  return x;
+}
+
+// Pull level: warp per 32 consecutive vertices. Light vertices (in-degree
+// <= kPullLight) are scanned by their own lane; heavy ones by the whole warp,
+// 32 in-edges per step with a warp-wide OR and an early exit once every
+// still-missing active source is found. Only sources whose frontier is not
+// empty at this level (ctl->srcmask) can reach anything new.
+constexpr int kPullLight = 32;
 __global__ void __launch_bounds__(kNT) k_ms_pull(MultiArgs a) {
-  __shared__ unsigned long long s_cnt, s_edges;
   Ctl *ctl = a.ctl;
   if (!ctl->active || ctl->mode != MODE_BITMAP) return;
   const uint32_t L = ctl->level;
+  const u64 active_src = ctl->srcmask[L & 1] & a.all;
   const u64 *Fc = cur_F(a, L);
   u64 *Fn = nxt_F(a, L);
   const int32_t V = a.g.V;
   const int32_t *coff = a.g.csc_offsets, *crow = a.g.csc_rows, *ro = a.g.row_offsets;
-  if (threadIdx.x == 0) {
-    s_cnt = 0;
-    s_edges = 0;
-  }
-  __syncthreads();
+  const int lane = lane_id();
   unsigned long long my_cnt = 0, my_edges = 0, my_bytes = 0;
-  for (int64_t v = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; v < V; v += (int64_t)gridDim.x * blockDim.x) {
-    const u64 vis = a.visit[v];
-    const u64 need = a.all & ~vis;
+  u64 act = 0;
+  const uint32_t groups = ((uint32_t)V + 31) / 32;
+  for (;;) {
+    // groups are handed out dynamically: a warp that drew a hub does not hold
+    // back the 32-vertex groups behind it
+    uint32_t grp = 0;
+    if (lane == 0) grp = atomicAdd(&ctl->group_ctr, 1u);
+    grp = __shfl_sync(0xffffffffu, grp, 0);
+    if (grp >= groups) break;
+    const int v = (int)(grp * 32 + lane);
+    const bool valid = v < V;
+    const u64 vis = valid ? a.visit[v] : ~0ull;
+    const u64 need = active_src & ~vis;
+    const int beg = valid ? coff[v] : 0, end = valid ? coff[v + 1] : 0;
     u64 acc = 0;
-    my_bytes += 16;  // visit read + next-mask write
-    if (need) {
-      const int beg = coff[v], end = coff[v + 1];
+    my_bytes += valid ? 16 : 0;  // visit read + next-mask write
+    const bool heavy = need && (end - beg) > kPullLight;
+    if (need && !heavy) {
+      // four in-edges per step: the row-index loads and then the four mask
+      // gathers are independent, so each lane keeps several loads in flight
       int e = beg;
-      for (; e < end; ++e) {
-        acc |= __ldg(&Fc[crow[e]]);
-        if ((acc & need) == need) {
-          ++e;
+      while (e < end) {
+        const int c = min(4, end - e);
+        const int u0 = crow[e];
+        const int u1 = c > 1 ? crow[e + 1] : u0;
+        const int u2 = c > 2 ? crow[e + 2] : u0;
+        const int u3 = c > 3 ? crow[e + 3] : u0;
+        acc |= __ldg(&Fc[u0]) | __ldg(&Fc[u1]) | __ldg(&Fc[u2]) | __ldg(&Fc[u3]);
+        e += c;
+        if ((acc & need) == need) break;
+      }
+      my_bytes += 8 + 12ull * (unsigned long long)(e - beg);  // offsets; row index + mask per edge
+    }
+    uint32_t hv = __ballot_sync(0xffffffffu, heavy);
+    while (hv) {
+      const int h = __ffs(hv) - 1;
+      hv &= hv - 1;
+      const u64 hneed = __shfl_sync(0xffffffffu, need, h);
+      const int hb = __shfl_sync(0xffffffffu, beg, h), he = __shfl_sync(0xffffffffu, end, h);
+      u64 hacc = 0;
+      int e0 = hb;
+      for (; e0 < he; e0 += 32) {
+        const int e = e0 + lane;
+        if (e < he) hacc |= __ldg(&Fc[crow[e]]);
+        hacc = warp_or(hacc);
+        if ((hacc & hneed) == hneed) {
+          e0 += 32;
           break;
         }
       }
-      my_bytes += 8 + 12ull * (unsigned long long)(e - beg);  // offsets; row index + mask per edge
-      acc &= need;
+      if (lane == h) {
+        acc = hacc;
+        my_bytes += 8 + 12ull * (unsigned long long)(min(e0, he) - hb);
+      }
     }
-    Fn[v] = acc;
+    acc &= need;
+    if (valid) Fn[v] = acc;
     if (acc) {
       my_bytes += 8 + 4ull * (unsigned long long)__popcll(acc);  // visit write + depths
       a.visit[v] = vis | acc;
-      write_bits(a.out + v * 64, acc, (int32_t)L + 1);
+      write_bits(a.out + (int64_t)v * 64, acc, (int32_t)L + 1);
       my_cnt += 1;
       my_edges += (unsigned long long)(ro[v + 1] - ro[v]);
+      act |= acc;
     }
   }
   add_bytes(ctl->kbytes, KID_MS_PULL, my_bytes);
+  act = warp_or(act);
+  if (lane == 0 && act) atomicOr(&ctl->srcmask[(L + 1) & 1], act);
+  // per-warp totals straight to the control block (no block barrier at the end)
   my_cnt = warp_sum(my_cnt);
   my_edges = warp_sum(my_edges);
-  if (lane_id() == 0 && (my_cnt || my_edges)) {
-    atomicAdd(&s_cnt, my_cnt);
-    atomicAdd(&s_edges, my_edges);
-  }
-  __syncthreads();
-  if (threadIdx.x == 0 && (s_cnt || s_edges)) {
-    atomicAdd((unsigned long long *)&ctl->acc[0], s_cnt);
-    atomicAdd(&ctl->next_edges, s_edges);
-  }
+  if (lane == 0 && my_cnt) atomicAdd((unsigned long long *)&ctl->acc[0], my_cnt);
+  if (lane == 0 && my_edges) atomicAdd(&ctl->next_edges, my_edges);
 }
 
 // Pull -> push: ordered compaction of the vertices with a non-empty mask into
@@ -282,6 +341,8 @@ __global__ void k_ms_level_end(Ctl *ctl, int32_t V, int64_t E, cudaGraphConditio
     } else {
       if ((double)n_next < (double)V / (double)ctl->beta && n_next < ctl->frontier_size) new_mode = MODE_QUEUE;
     }
+    ctl->srcmask[ctl->level & 1] = 0;  // consumed; the level after next accumulates it afresh
+    ctl->group_ctr = 0;
     ctl->apply_pending = (mode == MODE_QUEUE) ? 1u : 0u;
     ctl->convert = (mode == MODE_BITMAP && new_mode == MODE_QUEUE) ? 1u : 0u;
     ctl->mode = new_mode;
@@ -582,7 +643,7 @@ int mg_bfs_multi(mg_graph *g, const int32_t *srcs, int32_t nsrc, int32_t *depths
   const uint32_t max_iter = (uint32_t)std::min<int64_t>(o->iter_num > 0 ? o->iter_num : 0, g->nodes + 2);
   const int dir = o->direction;
   k_ctl_init<<<1, 32, 0, s>>>(g->ws.ctl, (uint32_t)distinct.size(), max_iter, (unsigned long long)o->spin_limit,
-                              dir == MG_DIR_PULL ? MODE_BITMAP : MODE_QUEUE);
+                              dir == MG_DIR_PULL ? MODE_BITMAP : MODE_QUEUE, ctl_flags(o));
   k_ms_init<<<1, 64, 0, s>>>(a, reinterpret_cast<const int32_t *>(g->ws.scan), nsrc);
   count_launch(2);
   // direction policy and switch factors in the control block
@@ -591,7 +652,7 @@ int mg_bfs_multi(mg_graph *g, const int32_t *srcs, int32_t nsrc, int32_t *depths
   struct {
     uint32_t dir;
     float alpha, beta;
-  } pol = {(uint32_t)dir, (float)o->alpha, (float)o->beta};
+  } pol = {(uint32_t)dir, (float)(o->alpha_multi > 0 ? o->alpha_multi : 5.0), (float)o->beta};
   cudaError_t e = cudaMemcpyAsync(&g->ws.ctl->dir_policy, &pol.dir, 4, cudaMemcpyHostToDevice, s);
   if (e == cudaSuccess) e = cudaMemcpyAsync(&g->ws.ctl->alpha, &pol.alpha, 4, cudaMemcpyHostToDevice, s);
   if (e == cudaSuccess) e = cudaMemcpyAsync(&g->ws.ctl->beta, &pol.beta, 4, cudaMemcpyHostToDevice, s);
@@ -650,7 +711,7 @@ int mg_sssp_multi(mg_graph *g, const int32_t *srcs, int32_t nsrc, int32_t *dists
   ga.gather_dir = NO_GATHER_EDGES;
   const uint32_t max_iter = (uint32_t)std::min<int64_t>(o->iter_num > 0 ? o->iter_num : 0, g->nodes + 2);
   k_ctl_init<<<1, 32, 0, s>>>(g->ws.ctl, (uint32_t)distinct.size(), max_iter, (unsigned long long)o->spin_limit,
-                              MODE_QUEUE);
+                              MODE_QUEUE, ctl_flags(o));
   k_mss_init<<<1, 64, 0, s>>>(a, reinterpret_cast<const int32_t *>(g->ws.scan), nsrc);
   count_launch(2);
   const int grid = persistent_grid(g, o, 4);

@@ -67,7 +67,12 @@ typedef struct mg_options {
   int32_t tile_items;        /* items per expand tile (0: autotuned) */
   int32_t ctas_per_sm;       /* persistent CTAs per SM (0: autotuned) */
   int32_t compute_stats;     /* 1: fill mg_stats.edges_traversed (one extra pass) */
-  int32_t reserved[7];
+  int32_t pad0;
+  double alpha_multi;        /* batched BFS: push->pull when the next level's frontier
+                                edges exceed edges / alpha_multi */
+  int32_t ordered_frontier;  /* 1: next frontiers keep a deterministic order (decoupled
+                                look-back); 0: one atomic reservation per tile */
+  int32_t reserved[3];
 } mg_options;
 
 /* Per-run statistics (reference: Statistics::stats_per_iter, GASengine/statistics.h:31-81). */

@@ -40,7 +40,7 @@ def test_bfs_multi_road_grid_and_duplicate_sources():
     out, st = g.bfs_multi(srcs)
     ref = np.stack([oracle.bfs(hg.row_offsets, hg.column_indices, s) for s in srcs])
     assert np.array_equal(out, ref)
-    assert st["iterations"] > 100
+    assert st["iterations"] >= int(ref.max())
 
 
 def test_bfs_multi_directed():

@@ -72,7 +72,13 @@ def test_bfs_host_loop_equals_graph_loop():
     s = hg.max_degree_vertex()
     a, _ = g.bfs(s, use_cuda_graph=1)
     b, _ = g.bfs(s, use_cuda_graph=0)
-    assert np.array_equal(a, b)
+    c, _ = g.bfs(s, ordered_frontier=1, direction=_lib.MG_DIR_PUSH)
+    assert np.array_equal(a, b) and np.array_equal(a, c)
+    hw = hg.with_weights(1, 64)
+    gw = Graph(hw)
+    d1, _ = gw.sssp(s, ordered_frontier=1)
+    d2, _ = gw.sssp(s, ordered_frontier=0)
+    assert np.array_equal(d1, d2)
 
 
 def test_bfs_roots_and_iter_limit():
