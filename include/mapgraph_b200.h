@@ -193,6 +193,18 @@ int mg_ppr_backward(mg_graph *g, const float *edge_weights, const float *ranks,
                     const float *grad_ranks, int32_t nvec, float *grad_edge_weights,
                     float *grad_teleport, mg_stats *stats, const mg_options *opts);
 
+/* BFS for callers that cannot allocate device memory (no counterpart in the
+ * reference). The graph (CSR row offsets and column indices, well formed) and
+ * the depths output are device pointers the caller owns; every working buffer
+ * lives in one static device array of about 14 MiB per GPU, so the call itself
+ * allocates nothing. Limits: nodes <= 2^20, edges <= 2^24 (MG_ERR_ARG beyond).
+ * Runs push levels only; results equal mg_bfs. The first call on a device looks
+ * up the array's device address, so make it before any stream capture. Calls
+ * share the array: calls that overlap on the GPU race and must be serialised.
+ * stream may be NULL (legacy default stream). */
+int mg_bfs_noalloc(const int32_t *d_row_offsets, const int32_t *d_column_indices, int64_t nodes,
+                   int64_t edges, int32_t src, int32_t *d_depths, void *stream, mg_stats *stats);
+
 /* -------------------------------------------------------------- builders -- */
 /* Seeded R-MAT generator (replaces the unseeded BuildRmatGraph,
  * b40c/graph/builder/rmat.cuh:145-224): edgefactor * 2^scale edges by recursive
