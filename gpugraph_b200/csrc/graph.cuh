@@ -85,6 +85,13 @@ struct mg_graph {
   unsigned long long *mask[3] = {nullptr, nullptr, nullptr};
   int32_t *multi_out = nullptr;         // [V][64] int32 per-source results
   size_t multi_bytes = 0;
+  // PageRank plan (built on first mg_pagerank): heavy in-lists split into
+  // fixed-size chunks whose partial sums are combined in chunk order.
+  int32_t *pr_chunk_v = nullptr, *pr_chunk_b = nullptr, *pr_chunk_e = nullptr;
+  int32_t *pr_heavy_v = nullptr, *pr_heavy_first = nullptr;
+  int32_t pr_nchunks = 0, pr_nheavy = 0;
+  int64_t pr_ndangling = 0;
+  float *pr_rank[2] = {nullptr, nullptr}, *pr_contrib[2] = {nullptr, nullptr}, *pr_partial = nullptr;
   size_t device_bytes = 0;
   uint64_t epochs_used = 0;  // look-back epochs consumed since the status words were cleared
   std::vector<void *> allocations;

@@ -217,12 +217,21 @@ __global__ void __launch_bounds__(kNT) k_ms_pull(MultiArgs a) {
       const int hb = __shfl_sync(0xffffffffu, beg, h), he = __shfl_sync(0xffffffffu, end, h);
       u64 hacc = 0;
       int e0 = hb;
-      for (; e0 < he; e0 += 32) {
-        const int e = e0 + lane;
-        if (e < he) hacc |= __ldg(&Fc[crow[e]]);
+      // 128 in-edges per step (four independent loads per lane), then one
+      // warp-wide OR and the early-exit test
+      for (; e0 < he; e0 += 128) {
+        int u[4];
+#pragma unroll
+        for (int j = 0; j < 4; ++j) {
+          const int e = e0 + 32 * j + lane;
+          u[j] = (e < he) ? crow[e] : -1;
+        }
+#pragma unroll
+        for (int j = 0; j < 4; ++j)
+          if (u[j] >= 0) hacc |= __ldg(&Fc[u[j]]);
         hacc = warp_or(hacc);
         if ((hacc & hneed) == hneed) {
-          e0 += 32;
+          e0 += 128;
           break;
         }
       }

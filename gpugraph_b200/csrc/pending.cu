@@ -4,9 +4,6 @@
 
 extern "C" {
 
-int mg_pagerank(mg_graph *, float *, mg_stats *, const mg_options *) {
-  return mg::set_error(MG_ERR_UNSUPPORTED, "mg_pagerank not built");
-}
 int mg_ppr_forward(mg_graph *, const float *, const float *, int32_t, float *, mg_stats *, const mg_options *) {
   return mg::set_error(MG_ERR_UNSUPPORTED, "mg_ppr_forward not built");
 }

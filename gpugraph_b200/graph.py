@@ -202,9 +202,11 @@ class Graph:
         out = np.empty(self.nodes, np.int32)
         return self._run(lib.mg_cc, "mg_cc", out, opts=default_options(**kw))
 
-    def pagerank(self, **kw):
+    def pagerank(self, damping: float = 0.85, tolerance: float = 1e-6, iter_num: int = 100, **kw):
+        """Normalised PageRank (FP32 ranks, FP64 norms); stops at L1 residual <= tolerance or iter_num."""
         out = np.empty(self.nodes, np.float32)
-        return self._run(lib.mg_pagerank, "mg_pagerank", out, opts=default_options(**kw))
+        return self._run(lib.mg_pagerank, "mg_pagerank", out,
+                         opts=default_options(damping=damping, tolerance=tolerance, iter_num=iter_num, **kw))
 
     def pagerank_gas(self, tolerance: float = 0.01, **kw):
         out = np.empty(self.nodes, np.float32)
