@@ -230,6 +230,9 @@ def run_native(args, rank: int, world: int):
         cms = ev0.elapsed_time(ev1)
         sub["cc"] = {"gedges_per_s": hg.edges / (cms * 1e-3) / 1e9, "ms": cms, "iterations": int(st.iterations)}
 
+    if not args.quick:
+        sub.update(extra_configs(dev, stream, hg.nodes))
+
     # ---- end to end through the C ABI with host buffers (pinned), one call per step
     host_out = torch.empty((NSRC, hg.nodes), dtype=torch.int32, pin_memory=True)
     o_host = _lib.default_options(stream=stream.cuda_stream, compute_stats=0)
@@ -266,6 +269,114 @@ def run_native(args, rank: int, world: int):
            "roofline": roofline, "clocks": clk.summary(), "V": hg.nodes, "E": hg.edges, "teps_edges": teps_edges}
     g.close()
     return res, hg, srcs
+
+
+def _time_events(fn, stream, reps=3):
+    import torch
+
+    fn()
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(reps):
+        fn()
+    e1.record(stream)
+    torch.cuda.synchronize()
+    return e0.elapsed_time(e1) / reps
+
+
+def extra_configs(dev, stream, _v22):
+    """The other workloads: PageRank (directed R-MAT 23 and the road grid), batched
+    BFS/SSSP on the road grid, the 256-graph batch and differentiable PPR."""
+    import ctypes as C
+
+    import torch
+
+    import gpugraph_b200 as gg
+    import oracle
+    from gpugraph_b200 import _lib
+
+    lib = _lib.lib
+    out = {}
+    st = _lib.Stats()
+    # PageRank: FP32 ranks vs the FP64 oracle at the same iteration count
+    for name, mk, directed in (("pagerank_rmat23", lambda: gg.HostGraph.rmat(23, 16, seed=SEED, symmetrize=False), True),
+                               ("pagerank_road1200", lambda: gg.HostGraph.road_grid(1200, 0.02, 0.005, seed=SEED),
+                                False)):
+        hg = mk()
+        g = gg.Graph(hg, directed=directed)
+        r = torch.empty(hg.nodes, dtype=torch.float32, device=dev)
+        o = _lib.default_options(outputs_on_device=1, iter_num=100, tolerance=1e-6, stream=stream.cuda_stream)
+        f = lambda: _lib.check(lib.mg_pagerank(g.handle, r.data_ptr(), C.byref(st), C.byref(o)), "mg_pagerank")
+        ms = _time_events(f, stream)
+        it = int(st.iterations)
+        t = hg.transpose() if directed else hg
+        ref, _, _ = oracle.pagerank_fp64(hg.row_offsets, t.row_offsets, t.column_indices, 0.85, 0.0, it)
+        diff = np.abs(r.cpu().numpy().astype(np.float64) - ref)
+        out[name] = {"gedges_per_s": hg.edges * it / (ms * 1e-3) / 1e9, "ms": ms, "iterations": it,
+                     "residual": float(st.residual), "l1_vs_fp64": float(diff.sum()), "maxabs_vs_fp64": float(diff.max()),
+                     "V": hg.nodes, "E": hg.edges}
+        g.close()
+    # batched 64-source BFS / SSSP on the road grid (uint32 weights in [1, 1000])
+    hg = gg.HostGraph.road_grid(1200, 0.02, 0.005, seed=SEED).with_weights(1, 1000, seed=SEED)
+    g = gg.Graph(hg)
+    srcs = pick_sources(hg, NSRC)
+    buf = torch.empty((NSRC, hg.nodes), dtype=torch.int32, device=dev)
+    one = torch.empty(hg.nodes, dtype=torch.int32, device=dev)
+    o = _lib.default_options(outputs_on_device=1, compute_stats=0, stream=stream.cuda_stream)
+    os_ = _lib.default_options(outputs_on_device=1, compute_stats=1, stream=stream.cuda_stream)
+    for algo, multi, single in (("bfs", lib.mg_bfs_multi, lib.mg_bfs), ("sssp", lib.mg_sssp_multi, lib.mg_sssp)):
+        _lib.check(multi(g.handle, srcs.ctypes.data, NSRC, buf.data_ptr(), C.byref(st), C.byref(os_)), algo)
+        teps = int(st.edges_traversed)
+        mms = _time_events(lambda: _lib.check(multi(g.handle, srcs.ctypes.data, NSRC, buf.data_ptr(), None,
+                                                    C.byref(o)), algo), stream, 2)
+        sms = _time_events(lambda: [_lib.check(single(g.handle, int(s), one.data_ptr(), None, C.byref(o)), algo)
+                                    for s in srcs[:8]], stream, 1) / 8 * NSRC
+        out[f"{algo}_road1200_batched64"] = {"gteps": teps / (mms * 1e-3) / 1e9, "ms": mms,
+                                             "single_x64_ms_est": sms, "batched_over_single": sms / mms}
+    g.close()
+    # 256 independent R-MAT graphs (scales U{10..16}, edgefactor 8), one BFS each, same launches
+    rng = np.random.default_rng(SEED)
+    graphs = [gg.HostGraph.rmat(int(s), 8, seed=1000 + i) for i, s in enumerate(rng.integers(10, 17, size=256))]
+    big = gg.concat_graphs(graphs)
+    gb = gg.Graph(big)
+    local = np.array([h.max_degree_vertex() for h in graphs], np.int32)
+    dep = torch.empty(big.nodes, dtype=torch.int32, device=dev)
+    _lib.check(lib.mg_bfs_batch(gb.handle, local.ctypes.data, dep.data_ptr(), C.byref(st), C.byref(os_)), "batch")
+    teps = int(st.edges_traversed)
+    bms = _time_events(lambda: _lib.check(lib.mg_bfs_batch(gb.handle, local.ctypes.data, dep.data_ptr(), None,
+                                                           C.byref(o)), "batch"), stream)
+    d = dep.cpu().numpy()
+    ok = all(np.array_equal(d[big.graph_offsets[i]:big.graph_offsets[i + 1]],
+                            oracle.bfs(graphs[i].row_offsets, graphs[i].column_indices, local[i])) for i in (0, 100, 255))
+    out["bfs_256_graph_batch"] = {"gteps": teps / (bms * 1e-3) / 1e9, "ms": bms, "graphs": 256, "V": big.nodes,
+                                  "E": big.edges, "spot_check_equal": ok}
+    gb.close()
+    # differentiable PPR: directed R-MAT 20, lognormal row-normalised weights, 32 teleport columns
+    from gpugraph_b200.ppr import ppr
+
+    hg = gg.HostGraph.rmat(20, 16, seed=SEED, symmetrize=False)
+    g = gg.Graph(hg, directed=True)
+    w = rng.lognormal(0.0, 1.0, size=hg.edges)
+    src = np.repeat(np.arange(hg.nodes), np.diff(hg.row_offsets))
+    w = w / np.bincount(src, weights=w, minlength=hg.nodes)[src]
+    T = np.zeros((hg.nodes, 32), np.float32)
+    for c in range(32):
+        T[rng.choice(hg.nodes, 100, replace=False), c] = 0.01
+    wt = torch.tensor(w, dtype=torch.float32, device=dev, requires_grad=True)
+    Tt = torch.tensor(T, device=dev, requires_grad=True)
+    Cm = torch.randn((hg.nodes, 32), device=dev)
+
+    def fb():
+        wt.grad = None
+        Tt.grad = None
+        (ppr(g, wt, Tt) * Cm).sum().backward()
+
+    fbms = _time_events(fb, stream, 2)
+    fms = _time_events(lambda: ppr(g, wt.detach(), Tt.detach()), stream, 2)
+    out["ppr_rmat20_32vec"] = {"forward_ms": fms, "forward_backward_ms": fbms, "V": hg.nodes, "E": hg.edges}
+    g.close()
+    return out
 
 
 # ---------------------------------------------------------- reference arm --

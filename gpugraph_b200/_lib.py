@@ -84,6 +84,7 @@ SIGNATURES = {
     "mg_profile_enable": (C.c_int, [C.c_int]),
     "mg_profile_read": (C.c_int, [C.c_int32, C.POINTER(C.c_char_p), C.POINTER(C.c_double), C.POINTER(C.c_int64),
                                   C.POINTER(C.c_uint64)]),
+    "mg_selftest_wait_timeout": (C.c_int, [C.c_int64, C.POINTER(C.c_double)]),
     "mg_graph_create": (C.c_int, [P, P, P, C.c_int32, C.c_int64, C.c_int64, C.c_int32, OPTP, C.POINTER(P)]),
     "mg_graph_create_batch": (C.c_int, [P, P, C.c_int64, C.c_int64, P, C.c_int32, OPTP, C.POINTER(P)]),
     "mg_graph_destroy": (C.c_int, [P]),

@@ -92,6 +92,17 @@ struct mg_graph {
   int32_t pr_nchunks = 0, pr_nheavy = 0;
   int64_t pr_ndangling = 0;
   float *pr_rank[2] = {nullptr, nullptr}, *pr_contrib[2] = {nullptr, nullptr}, *pr_partial = nullptr;
+  // Personalised PageRank: chunk plans over the CSC (forward) and the CSR
+  // (adjoint): chunk c covers edges [cb, ce) of vertex cv; cslot >= 0 marks a
+  // partial of a split in-list, combined in chunk order by the fix-up pass.
+  struct PprPlan {
+    int32_t *cv = nullptr, *cb = nullptr, *ce = nullptr, *cslot = nullptr;
+    int32_t *mv = nullptr, *mfirst = nullptr;  // split vertices and their first slot
+    int32_t nchunks = 0, nmulti = 0, nslots = 0;
+  } ppr_plan[2];
+  float *ppr_x[2] = {nullptr, nullptr}, *ppr_partial = nullptr;
+  float *ppr_rhs = nullptr, *ppr_w = nullptr;  // stable copies of the solve's inputs
+  int32_t ppr_cap_nvec = 0;
   size_t device_bytes = 0;
   uint64_t epochs_used = 0;  // look-back epochs consumed since the status words were cleared
   std::vector<void *> allocations;

@@ -114,6 +114,11 @@ int mg_profile_enable(int enable);
 /* Accumulated time, launch count and algorithmic bytes of kernel kind `kind`
  * (0 <= kind < 12); *name receives a static string. */
 int mg_profile_read(int32_t kind, const char **name, double *total_ms, int64_t *launches, uint64_t *bytes);
+/* Failure-detection self-test (no reference counterpart; the reference exits
+ * on errors, GASengine/enactor_vertex_centric.cuh:107-129): runs the library's
+ * bounded device-side wait against a status word nothing publishes. Returns
+ * MG_ERR_TIMEOUT when the wait ended at spin_limit as designed. */
+int mg_selftest_wait_timeout(int64_t spin_limit, double *elapsed_ms);
 
 /* ----------------------------------------------------------------- graphs -- */
 /* Copy a host CSR to the device and build what the hot path needs (out-degrees,
