@@ -450,44 +450,69 @@ __global__ void __launch_bounds__(kNT) k_mss_expand(MultiArgs a, const uint32_t 
       __syncthreads();
       break;
     }
+    // Four edges per warp step: the 8 lanes of group g relax edge k0+4s+g, lane
+    // `sub` owning sources 8*sub .. 8*sub+7, whose distances it reads with two
+    // 16-byte loads from each 256-byte row.
     const int k0 = warp * PER_WARP;
     const int k1 = min(cnt, k0 + PER_WARP);
-    for (int k = k0; k < k1; ++k) {
-      const int j = s_own[k];
-      const int el = k - s_base[j] - 1;
-      if (el < 0) continue;
-      const int u = s_v[j];
-      const int eid = s_rs[j] + el;
-      if ((unsigned)eid >= (unsigned)a.g.E) {
-        raise_error(ctl, MG_ERR_OVERFLOW);
-        continue;
-      }
-      const int v = col[eid];
-      const int w = wgt[eid];
-      const u64 am = Fc[u];
-      // column, weight, source mask; both distances of every active source
-      if (lane == 0) my_bytes += 16 + 8ull * (unsigned long long)__popcll(am);
-      const bool b0 = (am >> lane) & 1ull, b1 = (am >> (lane + 32)) & 1ull;
-      bool imp0 = false, imp1 = false;
-      if (b0 | b1) {
-        const int32_t *du = a.out + (int64_t)u * 64;
-        int32_t *dv = a.out + (int64_t)v * 64;
-        if (b0) {
-          const int c = du[lane] + w;
-          if (c < dv[lane]) imp0 = atomicMin(&dv[lane], c) > c;
+    const int grp = lane >> 3, sub = lane & 7;
+    for (int kb = k0; kb < k1; kb += 4) {
+      const int k = kb + grp;
+      int v = -1;
+      uint32_t imp = 0;
+      if (k < k1) {
+        const int j = s_own[k];
+        const int el = k - s_base[j] - 1;
+        if (el >= 0) {
+          const int u = s_v[j];
+          const int eid = s_rs[j] + el;
+          if ((unsigned)eid < (unsigned)a.g.E) {
+            v = col[eid];
+            const int w = wgt[eid];
+            const u64 am = Fc[u];
+            const uint32_t bits = (uint32_t)(am >> (8 * sub)) & 0xffu;
+            // column, weight, source mask; both distances of every active source
+            if (sub == 0) my_bytes += 16 + 8ull * (unsigned long long)__popcll(am);
+            if (bits) {
+              const int4 *pu = reinterpret_cast<const int4 *>(a.out + (int64_t)u * 64 + 8 * sub);
+              int32_t *dvp = a.out + (int64_t)v * 64 + 8 * sub;
+              const int4 *pv = reinterpret_cast<const int4 *>(dvp);
+              const int4 u0 = pu[0], u1 = pu[1], v0 = pv[0], v1 = pv[1];
+              const int du[8] = {u0.x, u0.y, u0.z, u0.w, u1.x, u1.y, u1.z, u1.w};
+              const int dv[8] = {v0.x, v0.y, v0.z, v0.w, v1.x, v1.y, v1.z, v1.w};
+#pragma unroll
+              for (int t = 0; t < 8; ++t) {
+                if ((bits >> t) & 1u) {
+                  const int c = du[t] + w;
+                  if (c < dv[t] && atomicMin(&dvp[t], c) > c) imp |= 1u << t;
+                }
+              }
+            }
+          } else {
+            raise_error(ctl, MG_ERR_OVERFLOW);
+          }
         }
-        if (b1) {
-          const int c = du[lane + 32] + w;
-          if (c < dv[lane + 32]) imp1 = atomicMin(&dv[lane + 32], c) > c;
-        }
       }
-      const u64 mask = (u64)__ballot_sync(0xffffffffu, imp0) | ((u64)__ballot_sync(0xffffffffu, imp1) << 32);
-      if (mask && lane == 0) {
+      // improved sources of the group's edge: OR of the 8 lanes' byte masks
+      u64 mask = (u64)imp << (8 * sub);
+      mask |= __shfl_xor_sync(0xffffffffu, mask, 1);
+      mask |= __shfl_xor_sync(0xffffffffu, mask, 2);
+      mask |= __shfl_xor_sync(0xffffffffu, mask, 4);
+      bool enq = false;
+      if (sub == 0 && mask) {
         my_bytes += 8 + 4ull * (unsigned long long)__popcll(mask);
         atomicOr(&Fn[v], mask);
         const uint32_t bit = 1u << (v & 31);
-        if (!(ld_volatile(&dedup[v >> 5]) & bit) && !(atomicOr(&dedup[v >> 5], bit) & bit)) {
-          const uint32_t pos = atomicAdd(&ctl->next_size, 1u);
+        enq = !(ld_volatile(&dedup[v >> 5]) & bit) && !(atomicOr(&dedup[v >> 5], bit) & bit);
+      }
+      // one queue reservation per warp step for its (up to four) new vertices
+      const uint32_t eb = __ballot_sync(0xffffffffu, enq);
+      if (eb) {
+        uint32_t base = 0;
+        if (lane == 0) base = atomicAdd(&ctl->next_size, (uint32_t)__popc(eb));
+        base = __shfl_sync(0xffffffffu, base, 0);
+        if (enq) {
+          const uint32_t pos = base + __popc(eb & lanemask_lt());
           if (pos < (uint32_t)V) Qn[pos] = v;
           else raise_error(ctl, MG_ERR_OVERFLOW);
         }
