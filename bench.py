@@ -58,25 +58,34 @@ class ClockSampler:
              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
 
-    def __init__(self, device_index: int = 0):
+    def __init__(self, device_index: int = 0, period_ms: int = 20):
         self.dev = device_index
+        self.period_ms = period_ms
         self.proc = None
-        self.lines: list[str] = []
+        self.lines: list[tuple[float, str]] = []  # (host arrival time, csv line)
+        self.window = None
 
     def __enter__(self):
         try:
             self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.dev}", f"--query-gpu={self.QUERY}",
-                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                          "--format=csv,noheader,nounits", "-lms", str(self.period_ms)],
                                          stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
             self.t = threading.Thread(target=self._read, daemon=True)
             self.t.start()
+            t_end = time.time() + 5.0
+            while not self.lines and time.time() < t_end:  # sampler is live before timing starts
+                time.sleep(0.01)
         except Exception:
             self.proc = None
         return self
 
     def _read(self):
         for line in self.proc.stdout:
-            self.lines.append(line.strip())
+            self.lines.append((time.time(), line.strip()))
+
+    def mark(self, t0: float, t1: float):
+        """Host times bracketing the timed region."""
+        self.window = (t0, t1)
 
     def __exit__(self, *exc):
         if self.proc:
@@ -89,7 +98,17 @@ class ClockSampler:
     def summary(self) -> dict:
         sm, mx, reasons = [], [], set()
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        for ln in self.lines:
+        lines, widened = [ln for _, ln in self.lines], 0
+        if self.window:
+            # samples taken during the timed region (one sampling period of slack
+            # for the arrival delay); widen only if the region was shorter than a period
+            for slack in (self.period_ms / 1000.0, 0.25, 0.5):
+                t0, t1 = self.window[0] - 0.0, self.window[1] + slack
+                sel = [ln for t, ln in self.lines if t0 <= t <= t1]
+                if sel:
+                    lines, widened = sel, int(slack * 1000)
+                    break
+        for ln in lines:
             f = [x.strip() for x in ln.split(",")]
             if len(f) < 9:
                 continue
@@ -104,7 +123,23 @@ class ClockSampler:
         if not sm:
             return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
         return {"sm_mhz": statistics.median(sm), "sm_max_mhz": max(mx), "reasons": sorted(reasons),
-                "samples": len(sm)}
+                "samples": len(sm), "window_slack_ms": widened, "period_ms": self.period_ms}
+
+
+def ncu_traffic(kernel: str):
+    """Per-launch DRAM bytes (read + write) of `kernel` at the bench workload, from
+    the committed ncu summary profiles/<kernel>__<workload>.md (line
+    'traffic_bytes_per_launch: N')."""
+    found = sorted((ROOT / "profiles").glob(f"{kernel}__*.md"))
+    if not found:
+        return None
+    for ln in found[0].read_text().splitlines():
+        if ln.startswith("traffic_bytes_per_launch:"):
+            try:
+                return float(ln.split(":", 1)[1].split()[0])
+            except ValueError:
+                return None
+    return None
 
 
 def measured_peak_hbm():
@@ -134,7 +169,8 @@ def run_native(args, rank: int, world: int):
     dev = torch.device("cuda")
     out_dev = torch.empty((NSRC, hg.nodes), dtype=torch.int32, device=dev)
     stream = torch.cuda.current_stream()
-    base_opts = dict(outputs_on_device=1, stream=stream.cuda_stream, compute_stats=0)
+    graphs = 0 if args.no_cuda_graph else 1
+    base_opts = dict(outputs_on_device=1, stream=stream.cuda_stream, compute_stats=0, use_cuda_graph=graphs)
     o_multi = _lib.default_options(**base_opts)
     st = _lib.Stats()
     src_arr = np.ascontiguousarray(srcs)
@@ -158,11 +194,13 @@ def run_native(args, rank: int, world: int):
         if world > 1:
             torch.distributed.barrier()
         torch.cuda.synchronize()
+        h0 = time.time()
         ev0.record(stream)
         for _ in range(args.steps):
             multi_step()
         ev1.record(stream)
         torch.cuda.synchronize()
+        clk.mark(h0, time.time())
         if world > 1:
             torch.distributed.barrier()
     launches = int(lib.mg_kernel_launches(1))
@@ -179,9 +217,12 @@ def run_native(args, rank: int, world: int):
     for s in srcs[:4]:
         _lib.check(lib.mg_bfs(g.handle, int(s), one.data_ptr(), None, o_single), "mg_bfs")
     torch.cuda.synchronize()
+    st1 = _lib.Stats()
+    dev_sum = 0.0
     ev0.record(stream)
     for s in srcs:
-        _lib.check(lib.mg_bfs(g.handle, int(s), one.data_ptr(), None, o_single), "mg_bfs")
+        _lib.check(lib.mg_bfs(g.handle, int(s), one.data_ptr(), st1, o_single), "mg_bfs")
+        dev_sum += float(st1.device_ms)
     ev1.record(stream)
     torch.cuda.synchronize()
     single_ms = ev0.elapsed_time(ev1)
@@ -194,8 +235,11 @@ def run_native(args, rank: int, world: int):
         parity &= bool(torch.equal(one, out_dev[k]))
 
     sub = {"bfs_batched64": {"gteps": value / world, "ms": ms_step, "levels": levels_multi},
-           "bfs_single_x64": {"gteps": single_gteps, "ms_total": single_ms, "ms_per_source": single_ms / NSRC},
+           "bfs_single_x64": {"gteps": single_gteps, "ms_total": single_ms, "ms_per_source": single_ms / NSRC,
+                              "device_ms_sum": dev_sum,
+                              "gteps_device_only": teps_edges / (dev_sum * 1e-3) / 1e9 if dev_sum else None},
            "batched_over_single": value / world / single_gteps,
+           "batched_over_single_device_only": (dev_sum / ms_step) if dev_sum else None,
            "batched_equals_single_spot_check": parity}
 
     # ---- SSSP: 8 sources one at a time (plain), and batched 64
@@ -235,7 +279,7 @@ def run_native(args, rank: int, world: int):
 
     # ---- end to end through the C ABI with host buffers (pinned), one call per step
     host_out = torch.empty((NSRC, hg.nodes), dtype=torch.int32, pin_memory=True)
-    o_host = _lib.default_options(stream=stream.cuda_stream, compute_stats=0)
+    o_host = _lib.default_options(stream=stream.cuda_stream, compute_stats=0, use_cuda_graph=graphs)
     src_pinned = torch.from_numpy(src_arr.copy()).pin_memory()
     _lib.check(lib.mg_bfs_multi(g.handle, src_pinned.data_ptr(), NSRC, host_out.data_ptr(), None, o_host), "e2e")
     torch.cuda.synchronize()
@@ -261,7 +305,7 @@ def run_native(args, rank: int, world: int):
         ms, n, byts = kernels[dom]
         achieved = byts / (ms * 1e-3) / 1e9 if ms > 0 else 0.0
         roofline = {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak, "unit": "GB/s",
-                    "frac": achieved / peak, "traffic": None, "peak_source": peak_kind,
+                    "frac": achieved / peak, "traffic": ncu_traffic(dom), "peak_source": peak_kind,
                     "launches": n, "bytes_per_launch": byts / max(n, 1), "ms_per_launch": ms / max(n, 1),
                     "kernels": {k: {"ms": v[0], "launches": v[1], "GB": v[2] / 1e9} for k, v in prof.items()}}
 
@@ -426,6 +470,8 @@ def main():
     ap.add_argument("--scale", type=int, default=SCALE)
     ap.add_argument("--quick", action="store_true", help="skip the SSSP/CC sub-results")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-cuda-graph", action="store_true",
+                    help="launch the same level kernels host-driven (for ncu launch lists)")
     args = ap.parse_args()
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))

@@ -102,6 +102,7 @@ SIGNATURES = {
     "mg_ppr_forward": (C.c_int, [P, P, P, C.c_int32, P, STP, OPTP]),
     "mg_ppr_backward": (C.c_int, [P, P, P, P, C.c_int32, P, P, STP, OPTP]),
     "mg_bfs_noalloc": (C.c_int, [P, P, C.c_int64, C.c_int64, C.c_int32, P, P, STP]),
+    "mg_autotune": (C.c_int, [P, C.c_int32, P, C.c_int32, OPTP, C.c_char_p, C.c_int64]),
     "mg_build_rmat": (C.c_int, [C.c_int32, C.c_int32, C.c_double, C.c_double, C.c_double, C.c_uint64, C.c_int32,
                                 C.c_int32, CSRP]),
     "mg_build_road_grid": (C.c_int, [C.c_int32, C.c_double, C.c_double, C.c_uint64, CSRP]),

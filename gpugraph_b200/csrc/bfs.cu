@@ -275,15 +275,23 @@ int bfs_run(mg_graph *g, const std::vector<int32_t> &roots, int32_t *depths, mg_
   if ((st = launch_check("bfs init kernels")) != MG_OK) return st;
   const int32_t Vv = g->csr.V;
   const int64_t E = g->edges;
+  // expand tile: 1024 or 2048 items (mg_options.tile_items; 0 = 2048)
+  const bool small_tiles = o->tile_items > 0 && o->tile_items <= 1024;
   LevelBody body = [=](cudaStream_t ss, cudaGraphConditionalHandle h, int use_h) {
     MG_LAUNCH(KID_CONVERT, ss, k_bm_to_queue<<<grid, kNT, 0, ss>>>(a));
-    MG_LAUNCH(KID_SCAN, ss, (k_frontier_scan<BfsP, kVTS, kVT><<<grid, kNT, 0, ss>>>(a)));
-    MG_LAUNCH(KID_EXPAND, ss, (k_expand<BfsP, kVT><<<grid, kNT, 0, ss>>>(a)));
+    if (small_tiles) {
+      MG_LAUNCH(KID_SCAN, ss, (k_frontier_scan<BfsP, kVTS, 4><<<grid, kNT, 0, ss>>>(a)));
+      MG_LAUNCH(KID_EXPAND, ss, (k_expand<BfsP, 4><<<grid, kNT, 0, ss>>>(a)));
+    } else {
+      MG_LAUNCH(KID_SCAN, ss, (k_frontier_scan<BfsP, kVTS, kVT><<<grid, kNT, 0, ss>>>(a)));
+      MG_LAUNCH(KID_EXPAND, ss, (k_expand<BfsP, kVT><<<grid, kNT, 0, ss>>>(a)));
+    }
     MG_LAUNCH(KID_BFS_PULL, ss, k_bfs_pull<<<grid, kNT, 0, ss>>>(a));
     MG_LAUNCH(KID_OTHER, ss, k_bfs_level_end<<<1, 32, 0, ss>>>(a.ctl, Vv, E, h, use_h));
   };
   LoopResult res;
-  st = run_level_loop(g, s, "bfs/" + std::to_string(grid), 5, body, o->use_cuda_graph != 0, &res);
+  st = run_level_loop(g, s, "bfs/" + std::to_string(grid) + (small_tiles ? "/t1024" : "/t2048"), 5, body,
+                      o->use_cuda_graph != 0, &res);
   if (st != MG_OK) return st;
   finish_run(g, res.ctl.level);
   if (res.ctl.error) return set_error(res.ctl.error, "bfs: device reported " + std::string(mg_status_string(res.ctl.error)));

@@ -67,15 +67,23 @@ int run_gas(mg_graph *g, const GasArgs<P> &a, uint32_t n0, const mg_options *o, 
   const int apply_all = P::applyOverEdges() == APPLY_ALL;
   const int post_all = P::postApplyOverEdges() == POST_APPLY_ALL;
   const int kpl = 3 + (gather ? 1 : 0) + (apply ? 1 : 0) + (post ? 1 : 0);
+  // expand tile: 1024 or 2048 items (mg_options.tile_items; 0 = 2048)
+  const bool small_tiles = o->tile_items > 0 && o->tile_items <= 1024;
   LevelBody body = [=](cudaStream_t ss, cudaGraphConditionalHandle h, int use_h) {
     if (gather) MG_LAUNCH(KID_GATHER, ss, k_gather<P><<<grid, kNT, 0, ss>>>(a));
     if (apply) MG_LAUNCH(KID_APPLY, ss, k_apply<P><<<grid, kNT, 0, ss>>>(a, apply_all, gather ? 1 : 0));
     if (post) MG_LAUNCH(KID_APPLY, ss, k_post_apply<P><<<grid, kNT, 0, ss>>>(a, post_all));
-    MG_LAUNCH(KID_SCAN, ss, (k_frontier_scan<P, kVTS, kVT><<<grid, kNT, 0, ss>>>(a)));
-    MG_LAUNCH(KID_EXPAND, ss, (k_expand<P, kVT><<<grid, kNT, 0, ss>>>(a)));
+    if (small_tiles) {
+      MG_LAUNCH(KID_SCAN, ss, (k_frontier_scan<P, kVTS, 4><<<grid, kNT, 0, ss>>>(a)));
+      MG_LAUNCH(KID_EXPAND, ss, (k_expand<P, 4><<<grid, kNT, 0, ss>>>(a)));
+    } else {
+      MG_LAUNCH(KID_SCAN, ss, (k_frontier_scan<P, kVTS, kVT><<<grid, kNT, 0, ss>>>(a)));
+      MG_LAUNCH(KID_EXPAND, ss, (k_expand<P, kVT><<<grid, kNT, 0, ss>>>(a)));
+    }
     MG_LAUNCH(KID_OTHER, ss, k_level_end<<<1, 32, 0, ss>>>(a.ctl, h, use_h));
   };
-  st = run_level_loop(g, s, std::string(name) + "/" + std::to_string(grid), kpl, body, o->use_cuda_graph != 0, res);
+  st = run_level_loop(g, s, std::string(name) + "/" + std::to_string(grid) + (small_tiles ? "/t1024" : "/t2048"),
+                      kpl, body, o->use_cuda_graph != 0, res);
   if (st != MG_OK) return st;
   finish_run(g, res->ctl.level);
   if (res->ctl.error)
