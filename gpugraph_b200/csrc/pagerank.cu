@@ -11,15 +11,16 @@
 // accumulates its |r' - r| and its dangling mass with Kahan compensation; only
 // the grid-wide residual and dangling reductions are FP64.
 //
-// Work split (deterministic sums): vertices with in-degree <= kPrHeavy are summed
-// by their own thread in CSC order; a CTA takes 256 consecutive vertices and
-// stages their 257 column offsets in shared memory with one TMA bulk copy.
-// Heavier in-lists are cut into kPrChunk-edge chunks, each summed by one warp
-// (lanes stride the chunk, then a fixed butterfly), and a fix-up pass adds a
-// vertex's chunk partials in chunk order. The next iteration's contributions
-// are written in the same pass that produces the ranks, so an iteration reads
-// the CSC once (4 bytes per edge) plus 4 bytes per edge of L2-resident
-// contribution gathers.
+// Work split (deterministic sums: the order of every addition depends only on
+// the graph): a warp takes 32 consecutive vertices and sweeps their contiguous
+// in-edges 32 at a time with a segmented warp scan, so the edge loads are
+// coalesced and balanced across the lanes whatever the in-degrees (a group of
+// short lists is summed lane by lane). In-lists longer than kPrBig are cut into
+// kPrChunk-edge chunks, each summed by one warp (lanes stride the chunk, then a
+// fixed butterfly), and a fix-up pass adds a vertex's chunk partials in chunk
+// order. The next iteration's contributions are written in the same pass that
+// produces the ranks, so an iteration reads the CSC once (4 bytes per edge)
+// plus 4 bytes per edge of L2-resident contribution gathers.
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -30,20 +31,21 @@
 #include "algo_util.cuh"
 #include "gas/driver.cuh"
 #include "gas/engine.cuh"
-#include "tma.cuh"
 
 namespace mg {
 
-constexpr int kPrHeavy = 32;
-constexpr int kPrChunk = 1024;
-constexpr int kPrTileV = kNT;  // vertices per light tile (one thread each)
+constexpr int kPrBig = 512;     // longer in-lists are summed by the chunk pass
+constexpr int kPrChunk = 1024;  // edges per chunk of a long in-list
+constexpr int kPrGroup = 32;    // vertices per warp group (one per lane)
+constexpr int kPrSub = 4;       // 32-edge sub-chunks whose loads are in flight together
+constexpr int kPrSerial = 8;    // a group whose lists are all this short is summed lane by lane
 
 struct PrArgs {
   const int32_t *coff, *crow;
   const float *inv;
   float *r0, *r1, *c0, *c1, *partial;
   const int32_t *chunk_v, *chunk_b, *chunk_e, *heavy_v, *heavy_first;
-  int32_t V, nchunks, nheavy, coff_len;
+  int32_t V, nchunks, nheavy;
   float damping;
   Ctl *ctl;
 };
@@ -55,14 +57,19 @@ MG_DEVINL void kahan_add(float &sum, float &comp, float x) {
   sum = t;
 }
 
-MG_DEVINL void pr_finalize(const PrArgs &a, int v, float s, float base, const float *rold, float *rnew, float *cnew,
-                           float &rs, float &rc, float &ds, float &dc) {
-  const float nr = fmaf(a.damping, s, base);
-  kahan_add(rs, rc, fabsf(nr - rold[v]));
-  const float iv = a.inv[v];
+// New rank of v from its in-edge sum s, given its old rank and 1/outdeg.
+MG_DEVINL void pr_store(float damping, int v, float s, float base, float r_old, float iv, float *rnew, float *cnew,
+                        float &rs, float &rc, float &ds, float &dc) {
+  const float nr = fmaf(damping, s, base);
+  kahan_add(rs, rc, fabsf(nr - r_old));
   if (iv == 0.f) kahan_add(ds, dc, nr);
   rnew[v] = nr;
   cnew[v] = nr * iv;
+}
+
+MG_DEVINL void pr_finalize(const PrArgs &a, int v, float s, float base, const float *rold, float *rnew, float *cnew,
+                           float &rs, float &rc, float &ds, float &dc) {
+  pr_store(a.damping, v, s, base, rold[v], a.inv[v], rnew, cnew, rs, rc, ds, dc);
 }
 
 // Reduces the per-thread compensated accumulators in FP64 into ctl->acc[1..2].
@@ -76,158 +83,128 @@ MG_DEVINL void pr_flush(Ctl *ctl, float rs, float rc, float ds, float dc) {
   }
 }
 
-// Issues the bulk copy of tile `tile`'s column offsets into buffer `buf`.
-MG_DEVINL void pr_stage_offsets(const PrArgs &a, uint32_t tile, int32_t *buf, uint64_t *bar) {
-  const int v0 = (int)tile * kPrTileV;
-  // offsets v0 .. v0+259, clamped to the padded array (both ends multiples of 4 entries)
-  const int n_off = min(kPrTileV + 4, a.coff_len - v0);
-  const uint32_t bytes = (uint32_t)n_off * 4u;
-  fence_proxy_async_smem();
-  mbar_arrive_expect_tx(bar, bytes);
-  bulk_copy_g2s(buf, a.coff + v0, bytes, bar);
+// One 32-edge sub-chunk [ck, ck+32) of a group sweep: lane i holds the
+// contribution of edge ck+i (0 outside the sweep). A segmented inclusive scan
+// with a head at every list start in the sub-chunk (and at lane 0) leaves the
+// sum of each list's part at its last lane; the list's owner lane adds it. A
+// step of offset d adds lane i-d's value into lane i when no head lies in
+// (i-d, i], a test on the head mask alone: with le = lanes [0, i], that window
+// is le & ~(le >> d), and for i < d it takes in lane 0, which is always a head.
+MG_DEVINL void pr_segment(float x, int ck, int b, int e, bool mine, uint32_t le, float &acc) {
+  const int p = b - ck;
+  const uint32_t head = __reduce_or_sync(0xffffffffu, (mine && p >= 0 && p < 32) ? 1u << p : 0u) | 1u;
+#pragma unroll
+  for (int d = 1; d < 32; d <<= 1) {
+    const float t = __shfl_up_sync(0xffffffffu, x, d);
+    if ((head & le & ~(le >> d)) == 0u) x += t;
+  }
+  const int q = min(e, ck + 32) - 1 - ck;
+  const float t = __shfl_sync(0xffffffffu, x, q < 0 ? 0 : (q > 31 ? 31 : q));
+  // the list has edges in this sub-chunk (an empty list has none anywhere)
+  if (mine && max(b, ck) < min(e, ck + 32)) acc += t;
 }
 
-constexpr int kPrTileEdges = kPrTileV * kPrHeavy;  // upper bound on a tile's light in-edges
-
-__global__ void __launch_bounds__(kNT) k_pr_iter(PrArgs a) {
-  __shared__ alignas(16) int32_t s_off[2][kPrTileV + 4];
-  __shared__ float s_val[kPrTileEdges];
-  __shared__ uint64_t s_bar[2];
-  __shared__ int s_ok;
+// Pull SpMV over warp groups of kPrGroup consecutive vertices (lane j owns
+// vertex v0+j). The warp sweeps the group's contiguous in-edge range in rounds
+// of kPrSub x 32 edges: coalesced row-index loads, then kPrSub independent
+// contribution gathers per lane, then one segmented warp scan per sub-chunk.
+// In-lists longer than kPrBig are skipped here (the chunk pass sums them), so
+// a group's sweep is at most kPrGroup * kPrBig edges. A group whose lists are
+// all at most kPrSerial long is summed lane by lane instead. Groups are dealt
+// round-robin to the grid's warps, and each warp loads its next group's
+// offsets while it sweeps the current one. No shared memory, no block
+// barriers. (Staging the 33 offsets of a group with a bulk copy on an
+// mbarrier measured slower than the two coalesced loads per lane.)
+__global__ void __launch_bounds__(kNT, 6) k_pr_iter(PrArgs a) {
   Ctl *ctl = a.ctl;
   if (!ctl->active) return;
   const uint32_t L = ctl->level;
   const float base = (float)ctl->dangling;
-  const unsigned long long spin_limit = ctl->spin_limit;
   const float *cold = (L & 1) ? a.c1 : a.c0;
   const float *rold = (L & 1) ? a.r1 : a.r0;
   float *rnew = (L & 1) ? a.r0 : a.r1;
   float *cnew = (L & 1) ? a.c0 : a.c1;
   float rs = 0.f, rc = 0.f, ds = 0.f, dc = 0.f;
   unsigned long long my_bytes = 0;
-  const uint32_t ntiles = ((uint32_t)a.V + kPrTileV - 1) / kPrTileV;
-  // Tiles are taken round-robin (every tile's work is bounded: a small tile
-  // holds <= kPrTileEdges edges, an oversized one only in-lists <= kPrHeavy),
-  // so the next tile is known without an atomic and its offsets are in flight
-  // while the current tile is summed.
-  if (threadIdx.x == 0) {
-    mbar_init(&s_bar[0], 1);
-    mbar_init(&s_bar[1], 1);
-    if (blockIdx.x < ntiles) pr_stage_offsets(a, blockIdx.x, s_off[0], &s_bar[0]);
+  const int lane = lane_id(), w = warp_id();
+  const uint32_t le = 0xffffffffu >> (31 - lane);  // lanes [0, lane]
+  const uint32_t ngroups = ((uint32_t)a.V + kPrGroup - 1) / kPrGroup;
+  const uint32_t nwarps = gridDim.x * kNW;
+  uint32_t grp = blockIdx.x * kNW + w;
+  // offsets of the next group, loaded one group ahead (lanes past the last
+  // vertex load nothing)
+  int nb = 0, ne = 0;
+  if (grp < ngroups && (int)(grp * kPrGroup) + lane < a.V) {
+    nb = a.coff[grp * kPrGroup + lane];
+    ne = a.coff[grp * kPrGroup + lane + 1];
   }
-  __syncthreads();
-  uint32_t tile = blockIdx.x;
-  uint32_t parity[2] = {0u, 0u};
-  int cur = 0;
-  while (tile < ntiles) {
-    __syncthreads();  // everyone has finished with the other buffer
-    const uint32_t par = parity[cur];
-    const uint32_t next = tile + gridDim.x;
-    if (threadIdx.x == 0) {
-      s_ok = mbar_wait_bounded(&s_bar[cur], par, spin_limit) ? 1 : 0;
-      if (!s_ok) {
-        // give the copy in flight one more bounded wait before leaving
-        mbar_wait_bounded(&s_bar[cur], par, spin_limit);
-      } else if (next < ntiles) {
-        // prefetch the next tile's offsets into the other buffer while this one is processed
-        pr_stage_offsets(a, next, s_off[cur ^ 1], &s_bar[cur ^ 1]);
-      }
+  for (; grp < ngroups; grp += nwarps) {
+    const int v0 = (int)grp * kPrGroup;
+    const int nv = min(kPrGroup, a.V - v0);
+    const bool valid = lane < nv;
+    const int b = nb, e = ne;
+    const int g_end = __shfl_sync(0xffffffffu, e, nv - 1);
+    int seg_b = __shfl_sync(0xffffffffu, b, 0);
+    const uint32_t next = grp + nwarps;
+    if (next < ngroups && (int)(next * kPrGroup) + lane < a.V) {
+      nb = a.coff[next * kPrGroup + lane];
+      ne = a.coff[next * kPrGroup + lane + 1];
     }
-    parity[cur] ^= 1u;
-    __syncthreads();
-    if (!s_ok) {
-      if (threadIdx.x == 0) raise_error(ctl, MG_ERR_TIMEOUT);
-      break;
-    }
-    // every thread observes the completed phase itself (acquire of the copy's writes)
-    if (!mbar_wait_bounded(&s_bar[cur], par, 1024)) raise_error(ctl, MG_ERR_TIMEOUT);
-    const int32_t *off = s_off[cur];
-    const int v0 = (int)tile * kPrTileV;
-    const int nv = min(kPrTileV, a.V - v0);
-    const int e_lo = off[0], e_hi = off[nv];
-    const bool small_tile = (e_hi - e_lo) <= kPrTileEdges;
-    if (small_tile) {
-      // phase 1: every thread strides the tile's whole edge range (coalesced
-      // row-index loads, eight independent gathers per step) into s_val
-      // rounds of 8 x kNT edges with predicated loads, so the tail of the
-      // range is not walked as a chain of dependent single loads
-      for (int k = e_lo + (int)threadIdx.x; k < e_hi; k += 8 * kNT) {
-        int u[8];
-        float x[8];
+    const bool big = valid && e - b > kPrBig;
+    const bool mine = valid && !big;
+    // the finalize inputs are independent of the sweep: load them first
+    const int v = v0 + lane;
+    const float r_old = mine ? rold[v] : 0.f, iv = mine ? a.inv[v] : 0.f;
+    float acc = 0.f;
+    if (__ballot_sync(0xffffffffu, valid && e - b > kPrSerial) == 0u) {
+      // every list of the group is short: each lane sums its own, all its
+      // loads in flight at once (CSC order)
+      int u[kPrSerial];
+      float x[kPrSerial];
 #pragma unroll
-        for (int j = 0; j < 8; ++j) u[j] = (k + j * kNT < e_hi) ? a.crow[k + j * kNT] : -1;
+      for (int k = 0; k < kPrSerial; ++k) u[k] = b + k < e ? a.crow[b + k] : -1;
 #pragma unroll
-        for (int j = 0; j < 8; ++j) x[j] = (u[j] >= 0) ? __ldg(&cold[u[j]]) : 0.f;
+      for (int k = 0; k < kPrSerial; ++k) x[k] = u[k] >= 0 ? __ldg(&cold[u[k]]) : 0.f;
 #pragma unroll
-        for (int j = 0; j < 8; ++j)
-          if (u[j] >= 0) s_val[k + j * kNT - e_lo] = x[j];
-      }
-    }
-    __syncthreads();
-    // phase 2: thread per vertex, sum in CSC order (deterministic). In a small
-    // tile, in-lists longer than kPrHeavy are summed by the whole warp from
-    // s_val (lanes stride the list, fixed butterfly); in an oversized tile they
-    // are left to the chunk pass.
-    const bool valid_v = (int)threadIdx.x < nv;
-    const int beg = valid_v ? off[threadIdx.x] : 0, end = valid_v ? off[threadIdx.x + 1] : 0;
-    if (small_tile) {
-      const int lane = lane_id();
-      uint32_t hv = __ballot_sync(0xffffffffu, valid_v && end - beg > kPrHeavy);
-      float hsum = 0.f;
-      while (hv) {
-        const int h = __ffs(hv) - 1;
-        hv &= hv - 1;
-        const int hb = __shfl_sync(0xffffffffu, beg, h) - e_lo, he = __shfl_sync(0xffffffffu, end, h) - e_lo;
-        float acc = 0.f;
-        for (int k = hb + lane; k < he; k += 32) acc += s_val[k];
+      for (int k = 0; k < kPrSerial; ++k) acc += x[k];
+    } else {
+    uint32_t pending = __ballot_sync(0xffffffffu, big);
+    for (;;) {
+      const int h = pending ? __ffs(pending) - 1 : -1;
+      const int seg_e = h >= 0 ? __shfl_sync(0xffffffffu, b, h) : g_end;
+      for (int c = seg_b; c < seg_e; c += kPrSub * 32) {
+        int u[kPrSub];
+        float x[kPrSub];
 #pragma unroll
-        for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
-        if (lane == h) hsum = acc;
-      }
-      if (valid_v) {
-        float s = 0.f;
-        if (end - beg > kPrHeavy) {
-          s = hsum;
-        } else {
-          for (int e = beg; e < end; ++e) s += s_val[e - e_lo];
+        for (int k = 0; k < kPrSub; ++k) {
+          const int i = c + 32 * k + lane;
+          u[k] = i < seg_e ? a.crow[i] : -1;
         }
-        pr_finalize(a, v0 + (int)threadIdx.x, s, base, rold, rnew, cnew, rs, rc, ds, dc);
-        my_bytes += 20 + 8ull * (unsigned long long)(end - beg);
+#pragma unroll
+        for (int k = 0; k < kPrSub; ++k) x[k] = u[k] >= 0 ? __ldg(&cold[u[k]]) : 0.f;
+#pragma unroll
+        for (int k = 0; k < kPrSub; ++k)
+          if (c + 32 * k < seg_e) pr_segment(x[k], c + 32 * k, b, e, mine, le, acc);
       }
-    } else if (valid_v) {
-      const int v = v0 + (int)threadIdx.x;
-      if (end - beg <= kPrHeavy) {
-        float s = 0.f;
-        {
-          int e = beg;
-          for (; e + 4 <= end; e += 4) {
-            const int u0 = a.crow[e], u1 = a.crow[e + 1], u2 = a.crow[e + 2], u3 = a.crow[e + 3];
-            const float x0 = __ldg(&cold[u0]), x1 = __ldg(&cold[u1]), x2 = __ldg(&cold[u2]), x3 = __ldg(&cold[u3]);
-            s += x0;
-            s += x1;
-            s += x2;
-            s += x3;
-          }
-          for (; e < end; ++e) s += __ldg(&cold[a.crow[e]]);
-        }
-        pr_finalize(a, v, s, base, rold, rnew, cnew, rs, rc, ds, dc);
-        my_bytes += 20 + 8ull * (unsigned long long)(end - beg);
-      }
+      if (h < 0) break;
+      pending &= pending - 1;
+      seg_b = __shfl_sync(0xffffffffu, e, h);
     }
-    tile = next;
-    cur ^= 1;
+    }
+    if (mine) {
+      pr_store(a.damping, v, acc, base, r_old, iv, rnew, cnew, rs, rc, ds, dc);
+      my_bytes += 20 + 8ull * (unsigned long long)(e - b);
+    }
   }
   // heavy chunks: warp per chunk, round-robin over the grid's warps (a chunk is
   // at most kPrChunk edges, and a shared atomic work counter would serialise
   // tens of thousands of warps on one address)
-  const int lane = lane_id();
-  const uint32_t nwarps = gridDim.x * kNW;
-  for (uint32_t c = blockIdx.x * kNW + warp_id(); c < (uint32_t)a.nchunks; c += nwarps) {
-    const int b = a.chunk_b[c], e = a.chunk_e[c];
+  for (uint32_t c = blockIdx.x * kNW + w; c < (uint32_t)a.nchunks; c += nwarps) {
+    const int cb = a.chunk_b[c], ce = a.chunk_e[c];
     float acc = 0.f;
-    int k = b + lane;
+    int k = cb + lane;
     // eight independent row-index loads, then eight independent gathers, per step
-    for (; k + 7 * 32 < e; k += 8 * 32) {
+    for (; k + 7 * 32 < ce; k += 8 * 32) {
       int u[8];
       float x[8];
 #pragma unroll
@@ -237,12 +214,12 @@ __global__ void __launch_bounds__(kNT) k_pr_iter(PrArgs a) {
 #pragma unroll
       for (int j = 0; j < 8; ++j) acc += x[j];
     }
-    for (; k < e; k += 32) acc += __ldg(&cold[a.crow[k]]);
+    for (; k < ce; k += 32) acc += __ldg(&cold[a.crow[k]]);
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
     if (lane == 0) {
       a.partial[c] = acc;
-      my_bytes += 4 + 8ull * (unsigned long long)(e - b);
+      my_bytes += 4 + 8ull * (unsigned long long)(ce - cb);
     }
   }
   add_bytes(ctl->kbytes, KID_PR_PULL, my_bytes);
@@ -313,12 +290,8 @@ static int pr_plan(mg_graph *g, cudaStream_t s) {
     inv[v] = od > 0 ? 1.0f / (float)od : 0.0f;
     ndang += od == 0;
     const int32_t b = co[v], en = co[v + 1];
-    // the same rule as k_pr_iter: a tile of kPrTileV vertices whose in-edges fit
-    // in shared memory is summed whole; in a larger tile, in-lists longer than
-    // kPrHeavy are chunked
-    const int64_t t0 = (v / kPrTileV) * kPrTileV, t1 = std::min<int64_t>(V, t0 + kPrTileV);
-    const bool small_tile = (int64_t)co[t1] - co[t0] <= kPrTileEdges;
-    if (!small_tile && en - b > kPrHeavy) {
+    // the same rule as k_pr_iter: in-lists longer than kPrBig are chunked
+    if (en - b > kPrBig) {
       hv.push_back((int32_t)v);
       hf.push_back((int32_t)cv.size());
       for (int32_t x = b; x < en; x += kPrChunk) {
@@ -403,7 +376,6 @@ extern "C" int mg_pagerank(mg_graph *g, float *ranks, mg_stats *stats, const mg_
   a.V = V;
   a.nchunks = g->pr_nchunks;
   a.nheavy = g->pr_nheavy;
-  a.coff_len = (int32_t)(((size_t)(V + 1 + 3) & ~(size_t)3) + 4);
   a.damping = (float)d;
   a.ctl = g->ws.ctl;
   k_pr_init<<<g->num_sms * 4, 256, 0, s>>>(a.inv, a.r0, a.c0, V, (float)inv_n);
@@ -412,7 +384,7 @@ extern "C" int mg_pagerank(mg_graph *g, float *ranks, mg_stats *stats, const mg_
   const double base0 = (1.0 - d) * inv_n + d * ((double)g->pr_ndangling * inv_n) * inv_n;
   cudaError_t e = cudaMemcpyAsync(&a.ctl->dangling, &base0, sizeof(double), cudaMemcpyHostToDevice, s);
   if ((st = cuda_status(e, "pagerank init")) != MG_OK) return st;
-  const int grid = persistent_grid(g, o, 6);  // 35 KB of shared memory per CTA: 6 fit on an SM
+  const int grid = persistent_grid(g, o, 6);  // 48 warps per SM (40 registers per thread)
   const int fix_grid = std::max(1, std::min(g->num_sms * 4, (g->pr_nheavy + kNT - 1) / kNT));
   const double tol = o->tolerance;
   LevelBody body = [=](cudaStream_t ss, cudaGraphConditionalHandle h, int use_h) {
