@@ -24,7 +24,7 @@ constexpr int kVTS = 4;  // frontier entries per thread in the scan
 constexpr int kVT = 8;   // items per thread in the expand (NV = 2048)
 
 // Bottom-up level: warp per 32-vertex bitmap word, lane per vertex.
-__global__ void __launch_bounds__(kNT) k_bfs_pull(GasArgs<BfsP> a) {
+__global__ void __launch_bounds__(kNT, 6) k_bfs_pull(GasArgs<BfsP> a) {
   Ctl *ctl = a.ctl;
   if (!ctl->active || ctl->mode != MODE_BITMAP) return;
   const uint32_t level = ctl->level;
@@ -36,12 +36,14 @@ __global__ void __launch_bounds__(kNT) k_bfs_pull(GasArgs<BfsP> a) {
   const int32_t *coff = a.g.csc_offsets, *crow = a.g.csc_rows, *ro = a.g.row_offsets;
   const int lane = lane_id();
   unsigned long long my_cnt = 0, my_edges = 0, my_bytes = 0;
+  // 32-vertex words are handed out dynamically (one atomic per word); the
+  // ticket for the next word is drawn while the current one is processed
+  uint32_t ticket = 0;
+  if (lane == 0) ticket = atomicAdd(&ctl->group_ctr, 1u);
   for (;;) {
-    // 32-vertex words are handed out dynamically (one atomic per word)
-    uint32_t w = 0;
-    if (lane == 0) w = atomicAdd(&ctl->group_ctr, 1u);
-    w = __shfl_sync(0xffffffffu, w, 0);
+    const uint32_t w = __shfl_sync(0xffffffffu, ticket, 0);
     if (w >= words) break;
+    if (lane == 0) ticket = atomicAdd(&ctl->group_ctr, 1u);
     const uint32_t vis = visited[w];
     const int v = (int)(w * 32 + lane);
     bool found = false;
@@ -267,6 +269,8 @@ int bfs_run(mg_graph *g, const std::vector<int32_t> &roots, int32_t *depths, mg_
   if (e == cudaSuccess) e = cudaMemsetAsync(w.bm[1], 0, w.words * 4, s);
   if ((st = cuda_status(e, "bfs init")) != MG_OK) return st;
   const int grid = persistent_grid(g, o, 4);
+  // the pull kernel holds no shared memory and at most 40 registers: 48 warps per SM
+  const int pull_grid = g->num_sms * 6;
   k_fill_i32<<<g->num_sms * 4, 256, 0, s>>>(w.vbuf[0], BfsP::INIT_VALUE, V);
   k_ctl_init<<<1, 32, 0, s>>>(w.ctl, nsrc, max_iter, (unsigned long long)o->spin_limit, MODE_QUEUE, ctl_flags(o));
   k_bfs_init<<<1, 256, 0, s>>>(w.ctl, w.queue[0], (int32_t)nsrc, w.vbuf[0], w.visited, w.bm[0], g->csr.row_offsets,
@@ -286,7 +290,7 @@ int bfs_run(mg_graph *g, const std::vector<int32_t> &roots, int32_t *depths, mg_
       MG_LAUNCH(KID_SCAN, ss, (k_frontier_scan<BfsP, kVTS, kVT><<<grid, kNT, 0, ss>>>(a)));
       MG_LAUNCH(KID_EXPAND, ss, (k_expand<BfsP, kVT><<<grid, kNT, 0, ss>>>(a)));
     }
-    MG_LAUNCH(KID_BFS_PULL, ss, k_bfs_pull<<<grid, kNT, 0, ss>>>(a));
+    MG_LAUNCH(KID_BFS_PULL, ss, k_bfs_pull<<<pull_grid, kNT, 0, ss>>>(a));
     MG_LAUNCH(KID_OTHER, ss, k_bfs_level_end<<<1, 32, 0, ss>>>(a.ctl, Vv, E, h, use_h));
   };
   LoopResult res;

@@ -159,13 +159,42 @@ MG_DEVINL u64 warp_or(u64 x) {
   return x;
 }
 
-// Pull level: warp per 32 consecutive vertices. Light vertices (in-degree
-// <= kPullLight) are scanned by their own lane; heavy ones by the whole warp,
-// 32 in-edges per step with a warp-wide OR and an early exit once every
-// still-missing active source is found. Only sources whose frontier is not
-// empty at this level (ctl->srcmask) can reach anything new.
-constexpr int kPullLight = 32;
-__global__ void __launch_bounds__(kNT) k_ms_pull(MultiArgs a) {
+constexpr int kMsSerial = 8;  // a group whose needed lists are all this short is pulled lane by lane
+constexpr int kMsSub = 4;     // 32-edge sub-chunks whose loads are in flight together
+
+// One 32-edge sub-chunk [ck, ck+32) of a group sweep: lane i holds the
+// frontier mask of edge ck+i's tail (0 when not loaded). A segmented inclusive
+// OR scan with a head at every non-empty list start in the sub-chunk (and at
+// lane 0) leaves the OR of each list's part at its last lane, which the list's
+// owner takes when it is still pulling. A step of offset d ORs lane i-d into
+// lane i when no head lies in (i-d, i]: with le = lanes [0, i] that window is
+// le & ~(le >> d), and for i < d it takes in lane 0, which is always a head.
+MG_DEVINL void ms_segment(u64 x, int ck, int b, int e, bool starts, bool take, uint32_t le, u64 &acc) {
+  const int p = b - ck;
+  const uint32_t head = __reduce_or_sync(0xffffffffu, (starts && p >= 0 && p < 32) ? 1u << p : 0u) | 1u;
+#pragma unroll
+  for (int d = 1; d < 32; d <<= 1) {
+    const u64 t = __shfl_up_sync(0xffffffffu, x, d);
+    if ((head & le & ~(le >> d)) == 0u) x |= t;
+  }
+  const int q = min(e, ck + 32) - 1 - ck;
+  const u64 t = __shfl_sync(0xffffffffu, x, q < 0 ? 0 : (q > 31 ? 31 : q));
+  if (take && max(b, ck) < min(e, ck + 32)) acc |= t;
+}
+
+// Pull level over warp groups of 32 consecutive vertices (lane j owns vertex
+// v0+j). A vertex pulls when an active source (ctl->srcmask: a source whose
+// frontier is not empty) has not reached it yet. If every pulling list of the
+// group has at most kMsSerial in-edges, each lane loads its whole list at once.
+// Otherwise the warp sweeps the pulling lists' contiguous in-edge range in
+// rounds of kMsSub x 32 edges (coalesced row-index loads, independent mask
+// gathers, a segmented OR scan per sub-chunk); after each round it drops the
+// lists that found every missing source or ended, and resumes at the first
+// list still pulling, so the early exit of the bottom-up step is kept at round
+// granularity while the loads stay coalesced and balanced across lanes. The
+// new depths of a vertex are written by the whole warp (lane l: sources l and
+// l+32 of its 256-byte row).
+__global__ void __launch_bounds__(kNT, 5) k_ms_pull(MultiArgs a) {
   Ctl *ctl = a.ctl;
   if (!ctl->active || ctl->mode != MODE_BITMAP) return;
   const uint32_t L = ctl->level;
@@ -175,80 +204,84 @@ __global__ void __launch_bounds__(kNT) k_ms_pull(MultiArgs a) {
   const int32_t V = a.g.V;
   const int32_t *coff = a.g.csc_offsets, *crow = a.g.csc_rows, *ro = a.g.row_offsets;
   const int lane = lane_id();
+  const uint32_t le = 0xffffffffu >> (31 - lane);  // lanes [0, lane]
   unsigned long long my_cnt = 0, my_edges = 0, my_bytes = 0;
   u64 act = 0;
   const uint32_t groups = ((uint32_t)V + 31) / 32;
+  // groups are handed out dynamically (a warp that drew a hub does not hold
+  // back the groups behind it); the ticket for the next group is drawn while
+  // the current one is processed
+  uint32_t ticket = 0;
+  if (lane == 0) ticket = atomicAdd(&ctl->group_ctr, 1u);
   for (;;) {
-    // groups are handed out dynamically: a warp that drew a hub does not hold
-    // back the 32-vertex groups behind it
-    uint32_t grp = 0;
-    if (lane == 0) grp = atomicAdd(&ctl->group_ctr, 1u);
-    grp = __shfl_sync(0xffffffffu, grp, 0);
+    const uint32_t grp = __shfl_sync(0xffffffffu, ticket, 0);
     if (grp >= groups) break;
-    const int v = (int)(grp * 32 + lane);
+    if (lane == 0) ticket = atomicAdd(&ctl->group_ctr, 1u);
+    const int v0 = (int)(grp * 32);
+    const int v = v0 + lane;
     const bool valid = v < V;
     const u64 vis = valid ? a.visit[v] : ~0ull;
     const u64 need = active_src & ~vis;
-    const int beg = valid ? coff[v] : 0, end = valid ? coff[v + 1] : 0;
-    u64 acc = 0;
+    const int b = valid ? coff[v] : 0, e = valid ? coff[v + 1] : 0;
     my_bytes += valid ? 16 : 0;  // visit read + next-mask write
-    const bool heavy = need && (end - beg) > kPullLight;
-    if (need && !heavy) {
-      // four in-edges per step: the row-index loads and then the four mask
-      // gathers are independent, so each lane keeps several loads in flight
-      int e = beg;
-      while (e < end) {
-        const int c = min(4, end - e);
-        const int u0 = crow[e];
-        const int u1 = c > 1 ? crow[e + 1] : u0;
-        const int u2 = c > 2 ? crow[e + 2] : u0;
-        const int u3 = c > 3 ? crow[e + 3] : u0;
-        acc |= __ldg(&Fc[u0]) | __ldg(&Fc[u1]) | __ldg(&Fc[u2]) | __ldg(&Fc[u3]);
-        e += c;
-        if ((acc & need) == need) break;
-      }
-      my_bytes += 8 + 12ull * (unsigned long long)(e - beg);  // offsets; row index + mask per edge
-    }
-    uint32_t hv = __ballot_sync(0xffffffffu, heavy);
-    while (hv) {
-      const int h = __ffs(hv) - 1;
-      hv &= hv - 1;
-      const u64 hneed = __shfl_sync(0xffffffffu, need, h);
-      const int hb = __shfl_sync(0xffffffffu, beg, h), he = __shfl_sync(0xffffffffu, end, h);
-      u64 hacc = 0;
-      int e0 = hb;
-      // 128 in-edges per step (four independent loads per lane), then one
-      // warp-wide OR and the early-exit test
-      for (; e0 < he; e0 += 128) {
-        int u[4];
+    const bool pulls = need != 0 && e > b;
+    u64 acc = 0;
+    unsigned long long probes = 0;
+    if (__ballot_sync(0xffffffffu, pulls && e - b > kMsSerial) == 0u) {
+      if (pulls) {
+        int u[kMsSerial];
 #pragma unroll
-        for (int j = 0; j < 4; ++j) {
-          const int e = e0 + 32 * j + lane;
-          u[j] = (e < he) ? crow[e] : -1;
+        for (int k = 0; k < kMsSerial; ++k) u[k] = b + k < e ? crow[b + k] : -1;
+#pragma unroll
+        for (int k = 0; k < kMsSerial; ++k)
+          if (u[k] >= 0) acc |= __ldg(&Fc[u[k]]);
+        probes = (unsigned long long)(e - b);
+      }
+    } else {
+      uint32_t pending = __ballot_sync(0xffffffffu, pulls);
+      const bool starts = valid && e > b;
+      int c = __shfl_sync(0xffffffffu, b, __ffs(pending) - 1);
+      for (;;) {
+        // one round from c; nothing past the last pulling list is loaded
+        const int lim = __shfl_sync(0xffffffffu, e, 31 - __clz(pending));
+        u64 x[kMsSub];
+#pragma unroll
+        for (int k = 0; k < kMsSub; ++k) {
+          const int i = c + 32 * k + lane;
+          x[k] = 0;
+          if (i < lim) {
+            x[k] = __ldg(&Fc[crow[i]]);
+            ++probes;
+          }
         }
 #pragma unroll
-        for (int j = 0; j < 4; ++j)
-          if (u[j] >= 0) hacc |= __ldg(&Fc[u[j]]);
-        hacc = warp_or(hacc);
-        if ((hacc & hneed) == hneed) {
-          e0 += 128;
-          break;
-        }
-      }
-      if (lane == h) {
-        acc = hacc;
-        my_bytes += 8 + 12ull * (unsigned long long)(min(e0, he) - hb);
+        for (int k = 0; k < kMsSub; ++k)
+          if (c + 32 * k < lim) ms_segment(x[k], c + 32 * k, b, e, starts, (pending >> lane) & 1u, le, acc);
+        c += kMsSub * 32;
+        // keep the lists that still miss a source and have edges left
+        pending = __ballot_sync(0xffffffffu, ((pending >> lane) & 1u) && (acc & need) != need && e > c);
+        if (!pending) break;
+        c = max(c, __shfl_sync(0xffffffffu, b, __ffs(pending) - 1));
       }
     }
+    my_bytes += pulls ? 8 + 12ull * probes : 0;  // offsets; row index + mask per probe
     acc &= need;
     if (valid) Fn[v] = acc;
     if (acc) {
       my_bytes += 8 + 4ull * (unsigned long long)__popcll(acc);  // visit write + depths
       a.visit[v] = vis | acc;
-      write_bits(a.out + (int64_t)v * 64, acc, (int32_t)L + 1);
       my_cnt += 1;
       my_edges += (unsigned long long)(ro[v + 1] - ro[v]);
       act |= acc;
+    }
+    uint32_t wv = __ballot_sync(0xffffffffu, acc != 0);
+    while (wv) {
+      const int j = __ffs(wv) - 1;
+      wv &= wv - 1;
+      const u64 m = __shfl_sync(0xffffffffu, acc, j);
+      int32_t *row = a.out + (int64_t)(v0 + j) * 64;
+      if ((m >> lane) & 1ull) row[lane] = (int32_t)L + 1;
+      if ((m >> (lane + 32)) & 1ull) row[lane + 32] = (int32_t)L + 1;
     }
   }
   add_bytes(ctl->kbytes, KID_MS_PULL, my_bytes);
@@ -695,6 +728,8 @@ int mg_bfs_multi(mg_graph *g, const int32_t *srcs, int32_t nsrc, int32_t *depths
     // The pull sweep reads the dense level-0 masks (already in F0).
   }
   const int grid = persistent_grid(g, o, 4);
+  // the pull kernel holds no shared memory and at most 48 registers: 40 warps per SM
+  const int pull_grid = g->num_sms * 5;
   const int32_t V = g->csr.V;
   const int64_t E = g->edges;
   LevelBody body = [=](cudaStream_t ss, cudaGraphConditionalHandle h, int use_h) {
@@ -702,7 +737,7 @@ int mg_bfs_multi(mg_graph *g, const int32_t *srcs, int32_t nsrc, int32_t *depths
     MG_LAUNCH(KID_CONVERT, ss, k_ms_convert<<<grid, kNT, 0, ss>>>(a));
     MG_LAUNCH(KID_SCAN, ss, (k_frontier_scan<msbfs_push, kMVTS, kMVT><<<grid, kNT, 0, ss>>>(ga)));
     MG_LAUNCH(KID_EXPAND, ss, (k_expand<msbfs_push, kMVT><<<grid, kNT, 0, ss>>>(ga)));
-    MG_LAUNCH(KID_MS_PULL, ss, k_ms_pull<<<grid, kNT, 0, ss>>>(a));
+    MG_LAUNCH(KID_MS_PULL, ss, k_ms_pull<<<pull_grid, kNT, 0, ss>>>(a));
     MG_LAUNCH(KID_OTHER, ss, k_ms_level_end<<<1, 32, 0, ss>>>(a.ctl, V, E, h, use_h));
   };
   LoopResult res;
