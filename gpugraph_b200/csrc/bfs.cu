@@ -33,7 +33,7 @@ __global__ void __launch_bounds__(kNT, 6) k_bfs_pull(GasArgs<BfsP> a) {
   uint32_t *visited = a.vl.d_visited;
   const int32_t V = a.g.V;
   const uint32_t words = ((uint32_t)V + 31) / 32;
-  const int32_t *coff = a.g.csc_offsets, *crow = a.g.csc_rows, *ro = a.g.row_offsets;
+  const int32_t *coff = a.g.csc_offsets, *crow = a.g.pull_rows, *ro = a.g.row_offsets;
   const int lane = lane_id();
   unsigned long long my_cnt = 0, my_edges = 0, my_bytes = 0;
   // 32-vertex words are handed out dynamically (one atomic per word); the

@@ -133,6 +133,7 @@ extern "C" int mg_bfs_noalloc(const int32_t *d_row_offsets, const int32_t *d_col
   a.g.col = const_cast<int32_t *>(d_column_indices);
   a.g.csc_offsets = a.g.row_offsets;
   a.g.csc_rows = a.g.col;
+  a.g.pull_rows = a.g.col;
   a.g.V = (int32_t)nodes;
   a.g.E = (int32_t)edges;
   a.vl.d_labels = d_depths;

@@ -97,6 +97,27 @@ using namespace mg;
 
 namespace {
 
+// Copy of the in-lists with every list ordered by descending out-degree of the
+// neighbour (ties by id), for the bottom-up kernels only: a high-degree
+// neighbour is the likeliest to be in the frontier, so their early exit comes
+// after fewer probes, and the hubs' frontier entries stay hot in cache. The
+// order of a list does not change which vertices a pull level finds.
+int upload_pull_rows(mg_graph *g, const int32_t *in_off, const int32_t *in_rows, const int32_t *row_offsets) {
+  const int64_t V = g->nodes, E = g->edges;
+  int st = device_alloc(g, (void **)&g->csr.pull_rows, (size_t)E * 4 + 64);
+  if (st != MG_OK || E == 0) return st;
+  std::vector<int32_t> pull(in_rows, in_rows + E);
+  host_parallel_for(V, [&](int64_t b, int64_t e, unsigned) {
+    for (int64_t v = b; v < e; ++v)
+      std::sort(pull.data() + in_off[v], pull.data() + in_off[v + 1], [&](int32_t x, int32_t y) {
+        const int32_t dx = row_offsets[x + 1] - row_offsets[x], dy = row_offsets[y + 1] - row_offsets[y];
+        return dx != dy ? dx > dy : x < y;
+      });
+  });
+  return cuda_status(cudaMemcpy(g->csr.pull_rows, pull.data(), (size_t)E * 4, cudaMemcpyHostToDevice),
+                     "pull list upload");
+}
+
 int create_common(const int32_t *row_offsets, const int32_t *col, const void *vals, int32_t value_type, int64_t nodes,
                   int64_t edges, int32_t directed, mg_graph **out) {
   if (!out) return set_error(MG_ERR_ARG, "out is NULL");
@@ -170,7 +191,8 @@ int create_common(const int32_t *row_offsets, const int32_t *col, const void *va
     e = cudaMemcpy(c.csc_offsets, t_off.data(), ro_n * 4, cudaMemcpyHostToDevice);
     if (e == cudaSuccess && E) e = cudaMemcpy(c.csc_rows, t_rows.data(), E * 4, cudaMemcpyHostToDevice);
     if (e == cudaSuccess && E) e = cudaMemcpy(c.csc_eid, t_eid.data(), E * 4, cudaMemcpyHostToDevice);
-    if ((st = cuda_status(e, "transpose upload")) != MG_OK) {
+    if ((st = cuda_status(e, "transpose upload")) != MG_OK ||
+        (st = upload_pull_rows(g, t_off.data(), t_rows.data(), row_offsets)) != MG_OK) {
       mg_graph_destroy(g);
       return st;
     }
@@ -180,6 +202,10 @@ int create_common(const int32_t *row_offsets, const int32_t *col, const void *va
     c.csc_offsets = c.row_offsets;
     c.csc_rows = c.col;
     c.csc_eid = nullptr;
+    if ((st = upload_pull_rows(g, row_offsets, col, row_offsets)) != MG_OK) {
+      mg_graph_destroy(g);
+      return st;
+    }
   }
   if ((st = ensure_workspace(g)) != MG_OK) {
     mg_graph_destroy(g);

@@ -9,6 +9,7 @@
 //   csc_offsets/csc_rows  transposed graph (in-edges); aliases the CSR when the
 //                         graph is symmetric
 //   csc_eid[E]            CSR edge id of every CSC entry (pull access to edge values)
+//   pull_rows[E]          the in-lists again, hubs first (bottom-up BFS only)
 //   out_degree_inv[V]     float 1/outdeg (PageRank), built on first use
 // The working set (queues, scan buffers, bitmaps, look-back status words) is
 // allocated once per graph and reused by every run on it.
@@ -31,6 +32,10 @@ struct DevCsr {
   int32_t *csc_offsets = nullptr;
   int32_t *csc_rows = nullptr;
   int32_t *csc_eid = nullptr;
+  // In-lists reordered by descending out-degree of the neighbour (ties by id),
+  // read only by the bottom-up kernels, whose early exit then comes sooner;
+  // shares csc_offsets.
+  int32_t *pull_rows = nullptr;
   int32_t V = 0;
   int32_t E = 0;
 };

@@ -202,7 +202,7 @@ __global__ void __launch_bounds__(kNT, 5) k_ms_pull(MultiArgs a) {
   const u64 *Fc = cur_F(a, L);
   u64 *Fn = nxt_F(a, L);
   const int32_t V = a.g.V;
-  const int32_t *coff = a.g.csc_offsets, *crow = a.g.csc_rows, *ro = a.g.row_offsets;
+  const int32_t *coff = a.g.csc_offsets, *crow = a.g.pull_rows, *ro = a.g.row_offsets;
   const int lane = lane_id();
   const uint32_t le = 0xffffffffu >> (31 - lane);  // lanes [0, lane]
   unsigned long long my_cnt = 0, my_edges = 0, my_bytes = 0;
