@@ -89,6 +89,7 @@ struct mg_graph {
   // Batched (mask-frontier) working set, allocated on first use.
   unsigned long long *mask[3] = {nullptr, nullptr, nullptr};
   int32_t *multi_out = nullptr;         // [V][64] int32 per-source results
+  int32_t *multi_stage = nullptr;       // [64][V] transposed results on their way to host memory
   size_t multi_bytes = 0;
   // PageRank plan (built on first mg_pagerank): heavy in-lists split into
   // fixed-size chunks whose partial sums are combined in chunk order.

@@ -98,14 +98,6 @@ MG_DEVINL u64 *nxt_F(const MultiArgs &a, uint32_t L) { return (L & 1) ? a.F0 : a
 MG_DEVINL int32_t *cur_Q(const MultiArgs &a, uint32_t L) { return (L & 1) ? a.q1 : a.q0; }
 MG_DEVINL int32_t *nxt_Q(const MultiArgs &a, uint32_t L) { return (L & 1) ? a.q0 : a.q1; }
 
-MG_DEVINL void write_bits(int32_t *row, u64 bits, int32_t value) {
-  while (bits) {
-    const int b = __ffsll((long long)bits) - 1;
-    bits &= bits - 1;
-    row[b] = value;
-  }
-}
-
 __global__ void k_ms_init(MultiArgs a, const int32_t *srcs, int32_t nsrc) {
   for (int s = threadIdx.x; s < nsrc; s += blockDim.x) {
     const int v = srcs[s];
@@ -129,17 +121,33 @@ __global__ void __launch_bounds__(kNT) k_ms_apply(MultiArgs a) {
   const int32_t *Q = cur_Q(a, L), *Qp = nxt_Q(a, L);
   u64 act = 0;
   unsigned long long my_bytes = 0;
-  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
-    const int v = Q[i];
-    const u64 vis = a.visit[v];
-    const u64 nb = Fc[v] & ~vis;
-    Fc[v] = nb;
-    act |= nb;
-    my_bytes += 28;  // queue entry, visit and mask read, mask write
-    if (nb) {
-      a.visit[v] = vis | nb;
-      write_bits(a.out + (int64_t)v * 64, nb, (int32_t)L);
-      my_bytes += 8 + 4ull * (unsigned long long)__popcll(nb);
+  const int lane = lane_id();
+  // whole warps walk the queue, so each new vertex's depths can be written by
+  // the warp together (lane l: sources l and l+32 of the 256-byte row)
+  const uint32_t n_pad = (n + 31) & ~31u;
+  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n_pad; i += gridDim.x * blockDim.x) {
+    int v = -1;
+    u64 nb = 0;
+    if (i < n) {
+      v = Q[i];
+      const u64 vis = a.visit[v];
+      nb = Fc[v] & ~vis;
+      Fc[v] = nb;
+      act |= nb;
+      my_bytes += 28;  // queue entry, visit and mask read, mask write
+      if (nb) {
+        a.visit[v] = vis | nb;
+        my_bytes += 8 + 4ull * (unsigned long long)__popcll(nb);
+      }
+    }
+    uint32_t wv = __ballot_sync(0xffffffffu, nb != 0);
+    while (wv) {
+      const int j = __ffs(wv) - 1;
+      wv &= wv - 1;
+      const u64 m = __shfl_sync(0xffffffffu, nb, j);
+      int32_t *row = a.out + (int64_t)__shfl_sync(0xffffffffu, v, j) * 64;
+      if ((m >> lane) & 1ull) row[lane] = (int32_t)L;
+      if ((m >> (lane + 32)) & 1ull) row[lane + 32] = (int32_t)L;
     }
   }
   for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < pn; i += gridDim.x * blockDim.x) {
@@ -402,19 +410,64 @@ __global__ void k_ms_level_end(Ctl *ctl, int32_t V, int64_t E, cudaGraphConditio
   if (use_handle) cudaGraphSetConditional(h, ctl->active);
 }
 
-// [V][64] -> [ns][V] for sources s_begin .. s_begin+ns-1, 32 vertices per tile
-// through shared memory (coalesced on both sides).
-__global__ void k_ms_transpose(const int32_t *in, int32_t *out, int32_t V, int32_t s_begin, int32_t ns) {
-  __shared__ int32_t t[32][65];
-  const int64_t v0 = (int64_t)blockIdx.x * 32;
-  for (int i = threadIdx.x; i < 32 * 64; i += blockDim.x) {
-    const int r = i / 64, c = i % 64;
-    t[r][c] = (v0 + r < V) ? in[(v0 + r) * 64 + c] : 0;
+// [V][64] -> [ns][V] for sources s_begin .. s_begin+ns-1. A CTA walks tiles of
+// kTrV vertices (grid-stride): 16-byte loads of the 256-byte rows into shared
+// memory, then each source's kTrV results leave as 128-byte coalesced stores.
+// With `visit` given (batched BFS), an entry whose visit bit is clear is
+// unreached: it comes out as -1, and its slot, which the traversal never
+// wrote, is not read (a row with no bits set is not read at all).
+constexpr int kTrV = 64;
+__global__ void __launch_bounds__(256) k_ms_transpose(const int32_t *in, const u64 *visit, int32_t *out, int32_t V,
+                                                      int32_t s_begin, int32_t ns) {
+  __shared__ int32_t t[kTrV][65];
+  const int64_t ntiles = ((int64_t)V + kTrV - 1) / kTrV;
+  const int lane = lane_id(), warp = warp_id();
+  for (int64_t tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
+    const int64_t v0 = tile * kTrV;
+    int4 q[kTrV * 16 / 256];
+#pragma unroll
+    for (int k = 0; k < kTrV * 16 / 256; ++k) {
+      const int idx = threadIdx.x + 256 * k, r = idx >> 4, c4 = idx & 15;
+      const int64_t v = v0 + r;
+      uint32_t bits = 0;
+      if (v < V) bits = visit ? (uint32_t)(visit[v] >> (4 * c4)) & 0xFu : 0xFu;
+      q[k] = bits ? *reinterpret_cast<const int4 *>(in + v * 64 + 4 * c4) : make_int4(-1, -1, -1, -1);
+      if (!(bits & 1u)) q[k].x = -1;
+      if (!(bits & 2u)) q[k].y = -1;
+      if (!(bits & 4u)) q[k].z = -1;
+      if (!(bits & 8u)) q[k].w = -1;
+    }
+    __syncthreads();  // the previous tile's rows have been written out
+#pragma unroll
+    for (int k = 0; k < kTrV * 16 / 256; ++k) {
+      const int idx = threadIdx.x + 256 * k, r = idx >> 4, c = 4 * (idx & 15);
+      t[r][c] = q[k].x;
+      t[r][c + 1] = q[k].y;
+      t[r][c + 2] = q[k].z;
+      t[r][c + 3] = q[k].w;
+    }
+    __syncthreads();
+    for (int seg = warp; seg < ns * (kTrV / 32); seg += kNW) {
+      const int s = seg / (kTrV / 32), r = (seg % (kTrV / 32)) * 32 + lane;
+      if (v0 + r < V) out[(int64_t)s * V + v0 + r] = t[r][s_begin + s];
+    }
   }
-  __syncthreads();
-  for (int i = threadIdx.x; i < 32 * ns; i += blockDim.x) {
-    const int s = i / 32, r = i % 32;
-    if (v0 + r < V) out[(int64_t)s * V + v0 + r] = t[r][s_begin + s];
+}
+
+// Reached (vertex, source) pairs and the out-edges of their vertices, from the
+// visit masks of a batched BFS.
+__global__ void k_ms_mask_stats(const u64 *visit, u64 all, const int32_t *ro, int32_t V, unsigned long long *out) {
+  unsigned long long cnt = 0, edg = 0;
+  for (int64_t v = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; v < V; v += (int64_t)gridDim.x * blockDim.x) {
+    const unsigned long long c = (unsigned long long)__popcll(visit[v] & all);
+    cnt += c;
+    edg += c * (unsigned long long)(ro[v + 1] - ro[v]);
+  }
+  cnt = warp_sum(cnt);
+  edg = warp_sum(edg);
+  if (lane_id() == 0) {
+    atomicAdd(&out[0], cnt);
+    atomicAdd(&out[1], edg);
   }
 }
 
@@ -611,11 +664,12 @@ static int multi_prepare(mg_graph *g, const int32_t *srcs, int32_t nsrc, const m
   if (e == cudaSuccess) e = cudaMemsetAsync(g->mask[2], 0, V * 8, s);
   if (e == cudaSuccess) e = cudaMemsetAsync(g->ws.bm[0], 0, g->ws.words * 4, s);
   if (e == cudaSuccess) e = cudaMemsetAsync(g->ws.bm[1], 0, g->ws.words * 4, s);
-  if (e == cudaSuccess && fill == -1) e = cudaMemsetAsync(g->multi_out, 0xff, V * 64 * 4, s);
   if (e == cudaSuccess) e = cudaMemcpyAsync(g->ws.queue[0], distinct->data(), distinct->size() * 4, cudaMemcpyHostToDevice, s);
   // the per-source source list goes in scan[] (free until the first scan)
   if (e == cudaSuccess) e = cudaMemcpyAsync(g->ws.scan, srcs, (size_t)nsrc * 4, cudaMemcpyHostToDevice, s);
   if ((st = cuda_status(e, "batched init")) != MG_OK) return st;
+  // batched BFS leaves the depth rows unset: the visit masks say which entries
+  // were written; batched SSSP relaxes with atomicMin from `fill`
   if (fill != -1) {
     k_fill_i32<<<g->num_sms * 8, 256, 0, s>>>(g->multi_out, fill, (int64_t)V * 64);
     count_launch();
@@ -629,6 +683,10 @@ static int multi_finish(mg_graph *g, cudaStream_t s, int32_t nsrc, int32_t *out,
   finish_run(g, res.ctl.level);
   if (res.ctl.error) return set_error(res.ctl.error, std::string("batched traversal: device reported ") +
                                                          mg_status_string(res.ctl.error));
+  // batched BFS (unreached == -1) reads reachability from the visit masks
+  const u64 *visit = unreached == -1 ? g->mask[0] : nullptr;
+  const u64 all = nsrc == 64 ? ~0ull : ((1ull << nsrc) - 1);
+  const int32_t V = g->csr.V;
   int st;
   if (stats) {
     stats->iterations = (int32_t)res.ctl.level;
@@ -638,29 +696,40 @@ static int multi_finish(mg_graph *g, cudaStream_t s, int32_t nsrc, int32_t *out,
     stats->device_ms = res.ms;
     stats->vertices_reached = 0;
     stats->edges_traversed = 0;
-    if (want_stats(o) &&
-        (st = reach_stats(g, s, g->multi_out, unreached, nsrc, 64, &stats->vertices_reached, &stats->edges_traversed)) !=
-            MG_OK)
-      return st;
+    if (want_stats(o)) {
+      if (visit) {
+        unsigned long long *acc = reinterpret_cast<unsigned long long *>(g->ws.ctl->acc);
+        unsigned long long h[2] = {0, 0};
+        cudaError_t e = cudaMemsetAsync(acc, 0, 16, s);
+        if (e == cudaSuccess) {
+          k_ms_mask_stats<<<g->num_sms * 4, 256, 0, s>>>(visit, all, g->csr.row_offsets, V, acc);
+          count_launch();
+          e = cudaMemcpyAsync(h, acc, 16, cudaMemcpyDeviceToHost, s);
+        }
+        if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+        if ((st = cuda_status(e, "batched stats")) != MG_OK) return st;
+        stats->vertices_reached = (int64_t)h[0];
+        stats->edges_traversed = (int64_t)h[1];
+      } else if ((st = reach_stats(g, s, g->multi_out, unreached, nsrc, 64, &stats->vertices_reached,
+                                   &stats->edges_traversed)) != MG_OK) {
+        return st;
+      }
+    }
   }
-  const int32_t V = g->csr.V;
-  const unsigned nblk = (unsigned)((V + 31) / 32);
+  const unsigned nblk = (unsigned)std::min<int64_t>((int64_t)g->num_sms * 8, ((int64_t)V + kTrV - 1) / kTrV);
   if (o->outputs_on_device) {
-    k_ms_transpose<<<nblk, 256, 0, s>>>(g->multi_out, out, V, 0, nsrc);
+    k_ms_transpose<<<nblk, 256, 0, s>>>(g->multi_out, visit, out, V, 0, nsrc);
     count_launch();
     return cuda_status(cudaStreamSynchronize(s), "batched result transpose");
   }
-  // Host output: transpose two sources at a time into the (now free) V x 8-byte
-  // mask buffers, rotating over the three so transposes overlap the copies.
-  for (int s0 = 0, c = 0; s0 < nsrc; s0 += 2, ++c) {
-    const int ns = std::min(2, nsrc - s0);
-    int32_t *buf = reinterpret_cast<int32_t *>(g->mask[c % 3]);
-    k_ms_transpose<<<nblk, 256, 0, s>>>(g->multi_out, buf, V, s0, ns);
-    count_launch();
-    cudaError_t e = cudaMemcpyAsync(out + (int64_t)s0 * V, buf, (size_t)ns * V * 4, cudaMemcpyDeviceToHost, s);
-    if (e != cudaSuccess) return cuda_status(e, "batched result copy");
-  }
-  return cuda_status(cudaStreamSynchronize(s), "batched result copy");
+  // Host output: transpose every source into a device staging buffer (kept for
+  // later runs), then one copy to the caller.
+  if (!g->multi_stage && (st = device_alloc(g, (void **)&g->multi_stage, (size_t)V * 64 * 4)) != MG_OK) return st;
+  k_ms_transpose<<<nblk, 256, 0, s>>>(g->multi_out, visit, g->multi_stage, V, 0, nsrc);
+  count_launch();
+  cudaError_t e = cudaMemcpyAsync(out, g->multi_stage, (size_t)nsrc * V * 4, cudaMemcpyDeviceToHost, s);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+  return cuda_status(e, "batched result copy");
 }
 
 }  // namespace mg
