@@ -166,7 +166,7 @@ static int build_graph(mg_graph *g, cudaStream_t s, const LevelBody &body, LoopC
 }
 
 int run_level_loop(mg_graph *g, cudaStream_t s, const std::string &key, int kernels_per_level, const LevelBody &body,
-                   bool use_graph, LoopResult *res) {
+                   bool use_graph, LoopResult *res, const std::function<void(cudaStream_t)> *epilogue) {
   cudaError_t e = cudaEventRecord(g->ev0, s);
   if (e != cudaSuccess) return cuda_status(e, "event record");
   bool graphed = false;
@@ -204,6 +204,11 @@ int run_level_loop(mg_graph *g, cudaStream_t s, const std::string &key, int kern
   }
   e = cudaEventRecord(g->ev1, s);
   if (e != cudaSuccess) return cuda_status(e, "event record");
+  if (epilogue) {
+    (*epilogue)(s);
+    int st = launch_check("loop epilogue");
+    if (st != MG_OK) return st;
+  }
   int st = read_ctl(g, s, &res->ctl);
   if (st != MG_OK) return st;
   prof_flush(s, res->ctl.kbytes);

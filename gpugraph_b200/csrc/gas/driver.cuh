@@ -26,8 +26,12 @@ struct LoopResult {
 
 // Runs the loop on stream s. kernels_per_level is used for launch accounting.
 // Events are recorded on s before the first and after the last level.
+// `epilogue`, when given, enqueues work that follows the loop on the same
+// stream before the control block is read back (one host synchronisation for
+// both); it is not part of the loop's measured time.
 int run_level_loop(mg_graph *g, cudaStream_t s, const std::string &key, int kernels_per_level,
-                   const LevelBody &body, bool use_graph, LoopResult *res);
+                   const LevelBody &body, bool use_graph, LoopResult *res,
+                   const std::function<void(cudaStream_t)> *epilogue = nullptr);
 
 // Persistent grid for the level-loop kernels.
 inline int persistent_grid(mg_graph *g, const mg_options *o, int default_per_sm) {

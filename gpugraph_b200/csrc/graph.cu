@@ -58,7 +58,7 @@ int ensure_workspace(mg_graph *g) {
     return st;
   MG_ALLOC(w.queue[0], V * 4);
   MG_ALLOC(w.queue[1], V * 4);
-  MG_ALLOC(w.scan, (V + 1 + 64) * 4);  // also stages up to 64 batched sources
+  MG_ALLOC(w.scan, (V + 1) * 4);
   MG_ALLOC(w.part, w.part_cap * 4);
   MG_ALLOC(w.status, w.status_cap * 8);
   MG_ALLOC(w.bm[0], w.words * 4);
@@ -78,7 +78,7 @@ int ensure_workspace(mg_graph *g) {
   return cuda_status(e, "workspace init");
 }
 
-int ensure_multi(mg_graph *g, bool need_dist) {
+int ensure_multi(mg_graph *g) {
   const size_t V = (size_t)g->nodes;
   int st;
   for (int i = 0; i < 3; ++i)
@@ -87,7 +87,6 @@ int ensure_multi(mg_graph *g, bool need_dist) {
     if ((st = device_alloc(g, (void **)&g->multi_out, V * 64 * 4)) != MG_OK) return st;
     g->multi_bytes = V * 64 * 4;
   }
-  (void)need_dist;
   return MG_OK;
 }
 

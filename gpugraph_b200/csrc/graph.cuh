@@ -119,7 +119,7 @@ namespace mg {
 // Library-internal helpers implemented in graph.cu.
 int device_alloc(mg_graph *g, void **p, size_t bytes);
 int ensure_workspace(mg_graph *g);
-int ensure_multi(mg_graph *g, bool need_dist);
+int ensure_multi(mg_graph *g);
 cudaStream_t run_stream(mg_graph *g, const mg_options *o);
 int cuda_status(cudaError_t e, const char *what);
 int launch_check(const char *what);

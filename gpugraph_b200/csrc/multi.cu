@@ -20,6 +20,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <cstring>
 #include <vector>
 
 #include "algo_util.cuh"
@@ -98,16 +99,33 @@ MG_DEVINL u64 *nxt_F(const MultiArgs &a, uint32_t L) { return (L & 1) ? a.F0 : a
 MG_DEVINL int32_t *cur_Q(const MultiArgs &a, uint32_t L) { return (L & 1) ? a.q1 : a.q0; }
 MG_DEVINL int32_t *nxt_Q(const MultiArgs &a, uint32_t L) { return (L & 1) ? a.q0 : a.q1; }
 
-__global__ void k_ms_init(MultiArgs a, const int32_t *srcs, int32_t nsrc) {
-  for (int s = threadIdx.x; s < nsrc; s += blockDim.x) {
-    const int v = srcs[s];
-    atomicOr(&a.F0[v], 1ull << s);
-    atomicOr(&a.visit[v], 1ull << s);
-    a.out[(int64_t)v * 64 + s] = 0;
+// A batched run's sources, passed by value to the init kernels (no host
+// staging copy): source s of the run is src[s]; the level-0 queue is the
+// sorted distinct list; dir/alpha/beta are the direction policy.
+struct SrcList {
+  int32_t src[64];
+  int32_t distinct[64];
+  int32_t nsrc, ndistinct;
+  uint32_t dir;
+  float alpha, beta;
+};
+
+// Level-0 state of a batched run (one CTA of 64 threads).
+__global__ void k_ms_init(MultiArgs a, SrcList L, int bfs) {
+  const int t = threadIdx.x;
+  if (t < L.nsrc) {
+    const int v = L.src[t];
+    atomicOr(&a.F0[v], 1ull << t);
+    if (bfs) atomicOr(&a.visit[v], 1ull << t);
+    a.out[(int64_t)v * 64 + t] = 0;
   }
-  if (threadIdx.x == 0) {
+  if (t < L.ndistinct) a.q0[t] = L.distinct[t];
+  if (t == 0 && bfs) {
     a.ctl->srcmask[0] = a.all;
     a.ctl->srcmask[1] = 0;
+    a.ctl->dir_policy = L.dir;
+    a.ctl->alpha = L.alpha;
+    a.ctl->beta = L.beta;
   }
 }
 
@@ -412,34 +430,42 @@ __global__ void k_ms_level_end(Ctl *ctl, int32_t V, int64_t E, cudaGraphConditio
 
 // [V][64] -> [ns][V] for sources s_begin .. s_begin+ns-1. A CTA walks tiles of
 // kTrV vertices (grid-stride): 16-byte loads of the 256-byte rows into shared
-// memory, then each source's kTrV results leave as 128-byte coalesced stores.
+// memory, then each source's kTrV results leave as 128-byte coalesced stores;
+// the next tile's loads are in flight while the current tile is written out.
 // With `visit` given (batched BFS), an entry whose visit bit is clear is
 // unreached: it comes out as -1, and its slot, which the traversal never
 // wrote, is not read (a row with no bits set is not read at all).
 constexpr int kTrV = 64;
-__global__ void __launch_bounds__(256) k_ms_transpose(const int32_t *in, const u64 *visit, int32_t *out, int32_t V,
+constexpr int kTrQ = kTrV * 16 / 256;  // 16-byte row pieces per thread per tile
+
+MG_DEVINL void tr_load(const int32_t *in, const u64 *visit, int32_t V, int64_t v0, int4 (&q)[kTrQ]) {
+#pragma unroll
+  for (int k = 0; k < kTrQ; ++k) {
+    const int idx = threadIdx.x + 256 * k, r = idx >> 4, c4 = idx & 15;
+    const int64_t v = v0 + r;
+    uint32_t bits = 0;
+    if (v < V) bits = visit ? (uint32_t)(visit[v] >> (4 * c4)) & 0xFu : 0xFu;
+    q[k] = bits ? *reinterpret_cast<const int4 *>(in + v * 64 + 4 * c4) : make_int4(-1, -1, -1, -1);
+    if (!(bits & 1u)) q[k].x = -1;
+    if (!(bits & 2u)) q[k].y = -1;
+    if (!(bits & 4u)) q[k].z = -1;
+    if (!(bits & 8u)) q[k].w = -1;
+  }
+}
+
+__global__ void __launch_bounds__(256, 6) k_ms_transpose(const int32_t *in, const u64 *visit, int32_t *out, int32_t V,
                                                       int32_t s_begin, int32_t ns) {
   __shared__ int32_t t[kTrV][65];
   const int64_t ntiles = ((int64_t)V + kTrV - 1) / kTrV;
   const int lane = lane_id(), warp = warp_id();
-  for (int64_t tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
+  int4 q[kTrQ];
+  int64_t tile = blockIdx.x;
+  if (tile < ntiles) tr_load(in, visit, V, tile * kTrV, q);
+  for (; tile < ntiles; tile += gridDim.x) {
     const int64_t v0 = tile * kTrV;
-    int4 q[kTrV * 16 / 256];
+    __syncthreads();  // the previous tile has been written out of t
 #pragma unroll
-    for (int k = 0; k < kTrV * 16 / 256; ++k) {
-      const int idx = threadIdx.x + 256 * k, r = idx >> 4, c4 = idx & 15;
-      const int64_t v = v0 + r;
-      uint32_t bits = 0;
-      if (v < V) bits = visit ? (uint32_t)(visit[v] >> (4 * c4)) & 0xFu : 0xFu;
-      q[k] = bits ? *reinterpret_cast<const int4 *>(in + v * 64 + 4 * c4) : make_int4(-1, -1, -1, -1);
-      if (!(bits & 1u)) q[k].x = -1;
-      if (!(bits & 2u)) q[k].y = -1;
-      if (!(bits & 4u)) q[k].z = -1;
-      if (!(bits & 8u)) q[k].w = -1;
-    }
-    __syncthreads();  // the previous tile's rows have been written out
-#pragma unroll
-    for (int k = 0; k < kTrV * 16 / 256; ++k) {
+    for (int k = 0; k < kTrQ; ++k) {
       const int idx = threadIdx.x + 256 * k, r = idx >> 4, c = 4 * (idx & 15);
       t[r][c] = q[k].x;
       t[r][c + 1] = q[k].y;
@@ -447,6 +473,7 @@ __global__ void __launch_bounds__(256) k_ms_transpose(const int32_t *in, const u
       t[r][c + 3] = q[k].w;
     }
     __syncthreads();
+    if (tile + gridDim.x < ntiles) tr_load(in, visit, V, (tile + gridDim.x) * kTrV, q);
     for (int seg = warp; seg < ns * (kTrV / 32); seg += kNW) {
       const int s = seg / (kTrV / 32), r = (seg % (kTrV / 32)) * 32 + lane;
       if (v0 + r < V) out[(int64_t)s * V + v0 + r] = t[r][s_begin + s];
@@ -625,14 +652,6 @@ __global__ void k_mss_level_end(Ctl *ctl, cudaGraphConditionalHandle h, int use_
   if (use_handle) cudaGraphSetConditional(h, ctl->active);
 }
 
-__global__ void k_mss_init(MultiArgs a, const int32_t *srcs, int32_t nsrc) {
-  for (int s = threadIdx.x; s < nsrc; s += blockDim.x) {
-    const int v = srcs[s];
-    atomicOr(&a.F0[v], 1ull << s);
-    a.out[(int64_t)v * 64 + s] = 0;
-  }
-}
-
 static MultiArgs multi_args(mg_graph *g) {
   MultiArgs a;
   a.g = g->csr;
@@ -651,12 +670,18 @@ static MultiArgs multi_args(mg_graph *g) {
 }
 
 static int multi_prepare(mg_graph *g, const int32_t *srcs, int32_t nsrc, const mg_options *o, cudaStream_t s,
-                         std::vector<int32_t> *distinct, int32_t fill) {
+                         SrcList *list, int32_t fill) {
   if (nsrc < 1 || nsrc > 64) return set_error(MG_ERR_ARG, "nsrc must be in [1, 64]");
-  int st = check_sources(g, srcs, nsrc, distinct);
+  std::vector<int32_t> distinct;
+  int st = check_sources(g, srcs, nsrc, &distinct);
   if (st != MG_OK) return st;
+  memset(list, 0, sizeof(*list));
+  std::copy(srcs, srcs + nsrc, list->src);
+  std::copy(distinct.begin(), distinct.end(), list->distinct);
+  list->nsrc = nsrc;
+  list->ndistinct = (int32_t)distinct.size();
   if ((st = ensure_workspace(g)) != MG_OK) return st;
-  if ((st = ensure_multi(g, true)) != MG_OK) return st;
+  if ((st = ensure_multi(g)) != MG_OK) return st;
   if ((st = prepare_run(g, s)) != MG_OK) return st;
   const size_t V = (size_t)g->nodes;
   cudaError_t e = cudaMemsetAsync(g->mask[0], 0, V * 8, s);
@@ -664,9 +689,6 @@ static int multi_prepare(mg_graph *g, const int32_t *srcs, int32_t nsrc, const m
   if (e == cudaSuccess) e = cudaMemsetAsync(g->mask[2], 0, V * 8, s);
   if (e == cudaSuccess) e = cudaMemsetAsync(g->ws.bm[0], 0, g->ws.words * 4, s);
   if (e == cudaSuccess) e = cudaMemsetAsync(g->ws.bm[1], 0, g->ws.words * 4, s);
-  if (e == cudaSuccess) e = cudaMemcpyAsync(g->ws.queue[0], distinct->data(), distinct->size() * 4, cudaMemcpyHostToDevice, s);
-  // the per-source source list goes in scan[] (free until the first scan)
-  if (e == cudaSuccess) e = cudaMemcpyAsync(g->ws.scan, srcs, (size_t)nsrc * 4, cudaMemcpyHostToDevice, s);
   if ((st = cuda_status(e, "batched init")) != MG_OK) return st;
   // batched BFS leaves the depth rows unset: the visit masks say which entries
   // were written; batched SSSP relaxes with atomicMin from `fill`
@@ -676,6 +698,19 @@ static int multi_prepare(mg_graph *g, const int32_t *srcs, int32_t nsrc, const m
   }
   (void)o;
   return MG_OK;
+}
+
+// Device output: the transpose runs as the level loop's epilogue, before the
+// control block is read back.
+static std::function<void(cudaStream_t)> transpose_epilogue(mg_graph *g, int32_t nsrc, int32_t *out, bool bfs) {
+  const u64 *visit = bfs ? g->mask[0] : nullptr;
+  const int32_t *in = g->multi_out;
+  const int32_t V = g->csr.V;
+  const unsigned nblk = (unsigned)std::min<int64_t>((int64_t)g->num_sms * 6, ((int64_t)V + kTrV - 1) / kTrV);  // 6 CTAs fit on an SM
+  return [=](cudaStream_t ss) {
+    k_ms_transpose<<<nblk, 256, 0, ss>>>(in, visit, out, V, 0, nsrc);
+    count_launch();
+  };
 }
 
 static int multi_finish(mg_graph *g, cudaStream_t s, int32_t nsrc, int32_t *out, int32_t unreached, mg_stats *stats,
@@ -716,12 +751,8 @@ static int multi_finish(mg_graph *g, cudaStream_t s, int32_t nsrc, int32_t *out,
       }
     }
   }
-  const unsigned nblk = (unsigned)std::min<int64_t>((int64_t)g->num_sms * 8, ((int64_t)V + kTrV - 1) / kTrV);
-  if (o->outputs_on_device) {
-    k_ms_transpose<<<nblk, 256, 0, s>>>(g->multi_out, visit, out, V, 0, nsrc);
-    count_launch();
-    return cuda_status(cudaStreamSynchronize(s), "batched result transpose");
-  }
+  if (o->outputs_on_device) return MG_OK;  // transposed by the loop's epilogue
+  const unsigned nblk = (unsigned)std::min<int64_t>((int64_t)g->num_sms * 6, ((int64_t)V + kTrV - 1) / kTrV);  // 6 CTAs fit on an SM
   // Host output: transpose every source into a device staging buffer (kept for
   // later runs), then one copy to the caller.
   if (!g->multi_stage && (st = device_alloc(g, (void **)&g->multi_stage, (size_t)V * 64 * 4)) != MG_OK) return st;
@@ -752,8 +783,8 @@ int mg_bfs_multi(mg_graph *g, const int32_t *srcs, int32_t nsrc, int32_t *depths
   mg_options d;
   const mg_options *o = opts_or_default(opts, &d);
   cudaStream_t s = run_stream(g, o);
-  std::vector<int32_t> distinct;
-  int st = multi_prepare(g, srcs, nsrc, o, s, &distinct, -1);
+  SrcList list;
+  int st = multi_prepare(g, srcs, nsrc, o, s, &list, -1);
   if (st != MG_OK) return st;
   MultiArgs a = multi_args(g);
   a.all = (nsrc == 64) ? ~0ull : ((1ull << nsrc) - 1);
@@ -778,24 +809,15 @@ int mg_bfs_multi(mg_graph *g, const int32_t *srcs, int32_t nsrc, int32_t *depths
   ga.gather_dir = NO_GATHER_EDGES;
   const uint32_t max_iter = (uint32_t)std::min<int64_t>(o->iter_num > 0 ? o->iter_num : 0, g->nodes + 2);
   const int dir = o->direction;
-  k_ctl_init<<<1, 32, 0, s>>>(g->ws.ctl, (uint32_t)distinct.size(), max_iter, (unsigned long long)o->spin_limit,
+  // direction policy and switch factors go to the control block with the sources
+  list.dir = (uint32_t)dir;
+  list.alpha = (float)(o->alpha_multi > 0 ? o->alpha_multi : 5.0);
+  list.beta = (float)o->beta;
+  k_ctl_init<<<1, 32, 0, s>>>(g->ws.ctl, (uint32_t)list.ndistinct, max_iter, (unsigned long long)o->spin_limit,
                               dir == MG_DIR_PULL ? MODE_BITMAP : MODE_QUEUE, ctl_flags(o));
-  k_ms_init<<<1, 64, 0, s>>>(a, reinterpret_cast<const int32_t *>(g->ws.scan), nsrc);
+  k_ms_init<<<1, 64, 0, s>>>(a, list, 1);
   count_launch(2);
-  // direction policy and switch factors in the control block
-  Ctl init_fields;
-  (void)init_fields;
-  struct {
-    uint32_t dir;
-    float alpha, beta;
-  } pol = {(uint32_t)dir, (float)(o->alpha_multi > 0 ? o->alpha_multi : 5.0), (float)o->beta};
-  cudaError_t e = cudaMemcpyAsync(&g->ws.ctl->dir_policy, &pol.dir, 4, cudaMemcpyHostToDevice, s);
-  if (e == cudaSuccess) e = cudaMemcpyAsync(&g->ws.ctl->alpha, &pol.alpha, 4, cudaMemcpyHostToDevice, s);
-  if (e == cudaSuccess) e = cudaMemcpyAsync(&g->ws.ctl->beta, &pol.beta, 4, cudaMemcpyHostToDevice, s);
-  if ((st = cuda_status(e, "batched bfs policy")) != MG_OK) return st;
-  if (dir == MG_DIR_PULL) {
-    // The pull sweep reads the dense level-0 masks (already in F0).
-  }
+  if ((st = launch_check("batched bfs init")) != MG_OK) return st;
   const int grid = persistent_grid(g, o, 4);
   // the pull kernel holds no shared memory and at most 48 registers: 40 warps per SM
   const int pull_grid = g->num_sms * 5;
@@ -810,11 +832,10 @@ int mg_bfs_multi(mg_graph *g, const int32_t *srcs, int32_t nsrc, int32_t *depths
     MG_LAUNCH(KID_OTHER, ss, k_ms_level_end<<<1, 32, 0, ss>>>(a.ctl, V, E, h, use_h));
   };
   LoopResult res;
-  st = run_level_loop(g, s, "bfs_multi/" + std::to_string(grid), 6, body, o->use_cuda_graph != 0, &res);
+  const auto epi = transpose_epilogue(g, nsrc, depths, true);
+  st = run_level_loop(g, s, "bfs_multi/" + std::to_string(grid), 6, body, o->use_cuda_graph != 0, &res,
+                      o->outputs_on_device ? &epi : nullptr);
   if (st != MG_OK) return st;
-  if (res.ctl.apply_pending && res.ctl.frontier_size == 0) {
-    // nothing left to apply: the last push level produced an empty queue
-  }
   return multi_finish(g, s, nsrc, depths, -1, stats, o, res);
 }
 
@@ -827,8 +848,8 @@ int mg_sssp_multi(mg_graph *g, const int32_t *srcs, int32_t nsrc, int32_t *dists
   mg_options d;
   const mg_options *o = opts_or_default(opts, &d);
   cudaStream_t s = run_stream(g, o);
-  std::vector<int32_t> distinct;
-  int st = multi_prepare(g, srcs, nsrc, o, s, &distinct, programs::sssp::INIT_VALUE);
+  SrcList list;
+  int st = multi_prepare(g, srcs, nsrc, o, s, &list, programs::sssp::INIT_VALUE);
   if (st != MG_OK) return st;
   MultiArgs a = multi_args(g);
   a.all = (nsrc == 64) ? ~0ull : ((1ull << nsrc) - 1);
@@ -848,10 +869,11 @@ int mg_sssp_multi(mg_graph *g, const int32_t *srcs, int32_t nsrc, int32_t *dists
   ga.expand_in = 0;
   ga.gather_dir = NO_GATHER_EDGES;
   const uint32_t max_iter = (uint32_t)std::min<int64_t>(o->iter_num > 0 ? o->iter_num : 0, g->nodes + 2);
-  k_ctl_init<<<1, 32, 0, s>>>(g->ws.ctl, (uint32_t)distinct.size(), max_iter, (unsigned long long)o->spin_limit,
+  k_ctl_init<<<1, 32, 0, s>>>(g->ws.ctl, (uint32_t)list.ndistinct, max_iter, (unsigned long long)o->spin_limit,
                               MODE_QUEUE, ctl_flags(o));
-  k_mss_init<<<1, 64, 0, s>>>(a, reinterpret_cast<const int32_t *>(g->ws.scan), nsrc);
+  k_ms_init<<<1, 64, 0, s>>>(a, list, 0);
   count_launch(2);
+  if ((st = launch_check("batched sssp init")) != MG_OK) return st;
   const int grid = persistent_grid(g, o, 4);
   uint32_t *scan = g->ws.scan;
   int32_t *part = g->ws.part;
@@ -862,7 +884,9 @@ int mg_sssp_multi(mg_graph *g, const int32_t *srcs, int32_t nsrc, int32_t *dists
     MG_LAUNCH(KID_OTHER, ss, k_mss_level_end<<<1, 32, 0, ss>>>(a.ctl, h, use_h));
   };
   LoopResult res;
-  st = run_level_loop(g, s, "sssp_multi/" + std::to_string(grid), 4, body, o->use_cuda_graph != 0, &res);
+  const auto epi = transpose_epilogue(g, nsrc, dists, false);
+  st = run_level_loop(g, s, "sssp_multi/" + std::to_string(grid), 4, body, o->use_cuda_graph != 0, &res,
+                      o->outputs_on_device ? &epi : nullptr);
   if (st != MG_OK) return st;
   return multi_finish(g, s, nsrc, dists, programs::sssp::INIT_VALUE, stats, o, res);
 }
