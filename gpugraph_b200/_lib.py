@@ -91,6 +91,7 @@ SIGNATURES = {
     "mg_graph_info": (C.c_int, [P, C.POINTER(C.c_int64), C.POINTER(C.c_int64), C.POINTER(C.c_int32),
                                 C.POINTER(C.c_int64)]),
     "mg_bfs": (C.c_int, [P, C.c_int32, P, STP, OPTP]),
+    "mg_bfs_pred": (C.c_int, [P, C.c_int32, P, P, STP, OPTP]),
     "mg_bfs_roots": (C.c_int, [P, P, C.c_int32, P, STP, OPTP]),
     "mg_bfs_multi": (C.c_int, [P, P, C.c_int32, P, STP, OPTP]),
     "mg_bfs_batch": (C.c_int, [P, P, P, STP, OPTP]),

@@ -91,6 +91,50 @@ __global__ void __launch_bounds__(kNT, 6) k_bfs_pull(GasArgs<BfsP> a) {
   if (lane == 0 && my_edges) atomicAdd(&ctl->next_edges, my_edges);
 }
 
+// Predecessors after a BFS, the rule of the reference's pred_extract
+// (Algorithms/BFS/predextract.cuh:143-154 gather_edge, :211-218 max reduce,
+// :236 empty in-lists): pred[v] = max(-1, max over in-neighbours u with
+// depth[v] - depth[u] == 1 of u). Depth arithmetic is kept as it is there, so a
+// root of a directed graph takes an unreached (-1) in-neighbour as its
+// predecessor. Warp per 32-vertex group: lists of up to 32 in-edges are scanned
+// by their own lane, longer ones by the whole warp (32 edges per step, then a
+// warp max). Unreached vertices (depth -1) cannot match and are not scanned.
+__global__ void __launch_bounds__(kNT) k_bfs_pred(const int32_t *coff, const int32_t *crow, const int32_t *depth,
+                                                  int32_t *pred, int32_t V) {
+  const int lane = lane_id();
+  const uint32_t groups = ((uint32_t)V + 31) / 32;
+  for (uint32_t grp = (blockIdx.x * blockDim.x + threadIdx.x) / 32; grp < groups;
+       grp += (gridDim.x * blockDim.x) / 32) {
+    const int v = (int)(grp * 32) + lane;
+    const bool valid = v < V;
+    const int dv = valid ? depth[v] : -1;
+    const int b = valid ? coff[v] : 0, e = valid ? coff[v + 1] : 0;
+    const bool scan = dv >= 0 && e > b;
+    int best = -1;
+    if (scan && e - b <= 32) {
+      for (int k = b; k < e; ++k) {
+        const int u = crow[k];
+        if (dv - depth[u] == 1) best = max(best, u);
+      }
+    }
+    uint32_t hv = __ballot_sync(0xffffffffu, scan && e - b > 32);
+    while (hv) {
+      const int h = __ffs(hv) - 1;
+      hv &= hv - 1;
+      const int hb = __shfl_sync(0xffffffffu, b, h), he = __shfl_sync(0xffffffffu, e, h);
+      const int hd = __shfl_sync(0xffffffffu, dv, h);
+      int m = -1;
+      for (int k = hb + lane; k < he; k += 32) {
+        const int u = crow[k];
+        if (hd - depth[u] == 1) m = max(m, u);
+      }
+      m = __reduce_max_sync(0xffffffffu, m);
+      if (lane == h) best = m;
+    }
+    if (valid) pred[v] = best;
+  }
+}
+
 // Pull -> push conversion at the start of a level: ordered compaction of the
 // frontier bitmap into the queue (decoupled look-back), and clearing of the
 // bitmap the coming push level will fill.
@@ -221,7 +265,9 @@ __global__ void k_bfs_init(Ctl *ctl, const int32_t *srcs, int32_t nsrc, int32_t 
 }
 
 // Shared by mg_bfs, mg_bfs_roots and mg_bfs_batch.
-int bfs_run(mg_graph *g, const std::vector<int32_t> &roots, int32_t *depths, mg_stats *stats, const mg_options *o) {
+// `preds` (optional): predecessors by the pred_extract rule (k_bfs_pred).
+int bfs_run(mg_graph *g, const std::vector<int32_t> &roots, int32_t *depths, mg_stats *stats, const mg_options *o,
+            int32_t *preds = nullptr) {
   mg_options dflt;
   if (!o) {
     mg_options_init(&dflt);
@@ -314,6 +360,12 @@ int bfs_run(mg_graph *g, const std::vector<int32_t> &roots, int32_t *depths, mg_
       stats->edges_traversed = ed;
     }
   }
+  if (preds) {
+    k_bfs_pred<<<g->num_sms * 8, kNT, 0, s>>>(g->csr.csc_offsets, g->csr.csc_rows, w.vbuf[0], w.vbuf[1], V);
+    count_launch();
+    if ((st = launch_check("bfs predecessors")) != MG_OK) return st;
+    if ((st = copy_out(s, preds, w.vbuf[1], (size_t)V * 4, o->outputs_on_device != 0)) != MG_OK) return st;
+  }
   return copy_out(s, depths, w.vbuf[0], (size_t)V * 4, o->outputs_on_device != 0);
 }
 
@@ -330,6 +382,16 @@ int mg_bfs(mg_graph *g, int32_t src, int32_t *depths, mg_stats *stats, const mg_
   int st = check_sources(g, &src, 1, &roots);
   if (st != MG_OK) return st;
   return bfs_run(g, roots, depths, stats, opts);
+}
+
+int mg_bfs_pred(mg_graph *g, int32_t src, int32_t *depths, int32_t *preds, mg_stats *stats, const mg_options *opts) {
+  clear_error();
+  if (!g) return set_error(MG_ERR_ARG, "graph is NULL");
+  if (!preds) return set_error(MG_ERR_ARG, "preds is NULL");
+  std::vector<int32_t> roots;
+  int st = check_sources(g, &src, 1, &roots);
+  if (st != MG_OK) return st;
+  return bfs_run(g, roots, depths, stats, opts, preds);
 }
 
 int mg_bfs_roots(mg_graph *g, const int32_t *srcs, int32_t nsrc, int32_t *depths, mg_stats *stats,

@@ -174,6 +174,15 @@ class Graph:
         out = np.empty(self.nodes, np.int32)
         return self._run(lib.mg_bfs, "mg_bfs", out, int(src), opts=default_options(**kw))
 
+    def bfs_pred(self, src: int, **kw):
+        """Depths and predecessors (pred_extract's rule: the largest in-neighbour one level up, else -1)."""
+        depths = np.empty(self.nodes, np.int32)
+        preds = np.empty(self.nodes, np.int32)
+        st = _lib.Stats()
+        check(lib.mg_bfs_pred(self._g, int(src), _ptr(depths), _ptr(preds), C.byref(st),
+                              C.byref(default_options(**kw))), "mg_bfs_pred")
+        return depths, preds, st.as_dict()
+
     def bfs_roots(self, srcs, **kw):
         s = np.ascontiguousarray(srcs, np.int32)
         out = np.empty(self.nodes, np.int32)

@@ -148,6 +148,12 @@ int mg_graph_info(const mg_graph *g, int64_t *nodes, int64_t *edges, int32_t *di
  * CsrProblem::ExtractResults (csr_problem.cuh:433-458). */
 int mg_bfs(mg_graph *g, int32_t src, int32_t *depths, mg_stats *stats,
            const mg_options *opts);
+/* mg_bfs plus predecessors, replacing pred_extract
+ * (Algorithms/BFS/predextract.cuh:246-375): preds[v] = the largest in-neighbour u
+ * with depths[v] - depths[u] == 1, else -1 (gather_edge :143-154, max reduce
+ * :211-218). preds has nodes entries, host or device like depths. */
+int mg_bfs_pred(mg_graph *g, int32_t src, int32_t *depths, int32_t *preds,
+                mg_stats *stats, const mg_options *opts);
 /* One BFS seeded with several roots at depth 0 (bfs::Initialize with num_srcs > 1,
  * bfs.h:62-79): depth = distance to the nearest root. */
 int mg_bfs_roots(mg_graph *g, const int32_t *srcs, int32_t nsrc, int32_t *depths,

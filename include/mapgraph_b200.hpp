@@ -39,7 +39,9 @@ struct pagerank {  // the reference PageRank program (unnormalised, |delta| thre
 };
 
 // The device-resident graph (reference: CsrProblem after FromHostProblem).
-template <class Program>
+// MARK_PREDECESSORS (the reference's template flag, GASengine/problem_type.cuh)
+// makes single-source BFS runs also produce predecessors for ExtractPreds.
+template <class Program, bool MARK_PREDECESSORS = false>
 class CsrProblem {
  public:
   CsrProblem() {
@@ -71,10 +73,19 @@ class CsrProblem {
     return MG_OK;
   }
 
+  // Copies the last run's predecessors (BFS with MARK_PREDECESSORS; the
+  // reference's CsrProblem::ExtractPreds, as called at Algorithms/BFS/bfs.cu:1063).
+  int ExtractPreds(int *h_preds) const {
+    if (preds_.empty()) return MG_ERR_ARG;
+    std::copy(preds_.begin(), preds_.end(), h_preds);
+    return MG_OK;
+  }
+
   mg_graph *graph() const { return g_; }
   mg_options &options() { return opts_; }
   int nodes() const { return nodes_; }
   std::vector<typename Program::DataType> &result() { return result_; }
+  std::vector<int> &preds() { return preds_; }
   const mg_stats &stats() const { return stats_; }
   mg_stats &stats() { return stats_; }
 
@@ -83,25 +94,34 @@ class CsrProblem {
   mg_options opts_;
   int nodes_ = 0;
   std::vector<typename Program::DataType> result_;
+  std::vector<int> preds_;
   mg_stats stats_{};
 };
 
 namespace detail {
-inline int run(CsrProblem<bfs> &p, int num_srcs, const int *srcs) {
+template <bool M>
+int run(CsrProblem<bfs, M> &p, int num_srcs, const int *srcs) {
   p.result().resize((size_t)p.nodes());
+  if (M && num_srcs == 1) {
+    p.preds().resize((size_t)p.nodes());
+    return mg_bfs_pred(p.graph(), srcs[0], p.result().data(), p.preds().data(), &p.stats(), &p.options());
+  }
   return num_srcs == 1 ? mg_bfs(p.graph(), srcs[0], p.result().data(), &p.stats(), &p.options())
                        : mg_bfs_roots(p.graph(), srcs, num_srcs, p.result().data(), &p.stats(), &p.options());
 }
-inline int run(CsrProblem<sssp> &p, int num_srcs, const int *srcs) {
+template <bool M>
+int run(CsrProblem<sssp, M> &p, int num_srcs, const int *srcs) {
   if (num_srcs != 1) return MG_ERR_UNSUPPORTED;  // the reference validates single-source runs only
   p.result().resize((size_t)p.nodes());
   return mg_sssp(p.graph(), srcs[0], p.result().data(), &p.stats(), &p.options());
 }
-inline int run(CsrProblem<cc> &p, int, const int *) {
+template <bool M>
+int run(CsrProblem<cc, M> &p, int, const int *) {
   p.result().resize((size_t)p.nodes());
   return mg_cc(p.graph(), p.result().data(), &p.stats(), &p.options());
 }
-inline int run(CsrProblem<pagerank> &p, int, const int *) {
+template <bool M>
+int run(CsrProblem<pagerank, M> &p, int, const int *) {
   p.result().resize((size_t)p.nodes());
   return mg_pagerank_gas(p.graph(), p.result().data(), &p.stats(), &p.options());
 }
@@ -115,7 +135,8 @@ class EnactorVertexCentric {
   // drivers (Algorithms/SSSP/sssp.cu:397-398): iter_num caps the GAS
   // iterations; threshold is the reference's expand switch (kept for API
   // compatibility: the load-balanced expand needs no threshold).
-  int EnactIterativeSearch(CsrProblem<Program> &problem, const int * /*h_row_offsets*/, int /*directed*/,
+  template <bool M>
+  int EnactIterativeSearch(CsrProblem<Program, M> &problem, const int * /*h_row_offsets*/, int /*directed*/,
                            int num_srcs, const int *srcs, int iter_num, int threshold) {
     if (iter_num > 0) problem.options().iter_num = iter_num;
     problem.options().threshold = threshold;

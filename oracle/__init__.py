@@ -40,6 +40,7 @@ def _load():
     lib.oracle_cc_push.argtypes = [_I64, _P, _P, _P]
     lib.oracle_pr_gas.argtypes = [_I64, _P, _P, _P, _P, _P, C.c_float, C.c_int32, _P, _P]
     lib.oracle_pagerank_fp64.argtypes = [_I64, _P, _P, _P, C.c_double, C.c_double, C.c_int32, _P, _P, _P]
+    lib.oracle_bfs_pred.argtypes = [_I64, _P, _P, _P, _P]
     return lib
 
 
@@ -81,6 +82,14 @@ def bfs(ro, col, srcs) -> np.ndarray:
     s = _c32(np.atleast_1d(srcs))
     out = np.empty(len(ro) - 1, np.int32)
     assert lib().oracle_bfs(len(ro) - 1, _p(ro), _p(col), _p(s), len(s), _p(out)) == 0
+    return out
+
+
+def bfs_pred(coff, crow, depth) -> np.ndarray:
+    """Predecessors from BFS depths by pred_extract's rule (coff/crow: in-lists)."""
+    coff, crow, depth = _c32(coff), _c32(crow), _c32(depth)
+    out = np.empty(len(coff) - 1, np.int32)
+    assert lib().oracle_bfs_pred(len(coff) - 1, _p(coff), _p(crow), _p(depth), _p(out)) == 0
     return out
 
 

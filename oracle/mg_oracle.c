@@ -267,3 +267,21 @@ int oracle_pagerank_fp64(int64_t n, const int32_t *ro, const int32_t *coff, cons
   free(contrib);
   return 0;
 }
+
+/* pred_extract (Algorithms/BFS/predextract.cuh:246-375): for every vertex, the
+ * in-edges' gather_edge values (:143-154: the in-neighbour u when
+ * depth[v] - depth[u] == 1, else -1) reduced with max (ReduceFunctor :211-218)
+ * from INIT_VALUE -1, so a vertex without such an in-neighbour (or without
+ * in-edges, :236) gets -1. coff/crow: the in-lists (CSC). */
+int oracle_bfs_pred(int64_t n, const int32_t *coff, const int32_t *crow, const int32_t *depth, int32_t *pred) {
+  for (int64_t v = 0; v < n; ++v) {
+    int32_t best = -1;
+    for (int32_t j = coff[v]; j < coff[v + 1]; ++j) {
+      const int32_t u = crow[j];
+      const int32_t val = (depth[v] - depth[u]) == 1 ? u : -1;
+      if (val > best) best = val;
+    }
+    pred[v] = best;
+  }
+  return 0;
+}

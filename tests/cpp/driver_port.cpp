@@ -39,8 +39,28 @@ static int run(const char *name, const int *vals, int directed, bool print_int) 
   return MG_OK;
 }
 
+// BFS with predecessors (MARK_PREDECESSORS), printed as "bfs_pred" + preds.
+static int run_pred() {
+  mapgraph::CsrProblem<mapgraph::bfs, true> problem;
+  int st = problem.FromHostProblem(false, 7, 11, kCol, kRow, nullptr, nullptr, nullptr, 1, 1);
+  mapgraph::EnactorVertexCentric<mapgraph::bfs> enactor;
+  int src = 0;
+  if (st == MG_OK) st = enactor.EnactIterativeSearch(problem, kRow, 1, 1, &src, 1 << 30, 0);
+  std::vector<int> preds(7);
+  if (st == MG_OK) st = problem.ExtractPreds(preds.data());
+  if (st != MG_OK) {
+    std::printf("bfs_pred failed: %s\n", mapgraph::LastError().c_str());
+    return st;
+  }
+  std::printf("bfs_pred");
+  for (int x : preds) std::printf(" %d", x);
+  std::printf("\n");
+  return MG_OK;
+}
+
 int main() {
   int st = run<mapgraph::bfs>("bfs", nullptr, 1, true);
+  st |= run_pred();
   st |= run<mapgraph::sssp>("sssp", kVal, 1, true);
   st |= run<mapgraph::cc>("cc", nullptr, 1, true);
   st |= run<mapgraph::pagerank>("pagerank", nullptr, 1, false);

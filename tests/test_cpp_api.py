@@ -33,3 +33,14 @@ def test_cpp_driver_matches_reference_cpu_results(tmp_path):
     assert [int(x) for x in got["bfs"]] == ex["bfs"]["0"]
     assert [int(x) for x in got["sssp"]] == ex["sssp"]["0"]
     assert len(got["pagerank"]) == 7 and len(got["cc"]) == 7
+    # predecessors by pred_extract's rule, from the oracle on the same directed graph
+    import numpy as np
+
+    import oracle
+    from gpugraph_b200 import HostGraph
+
+    fx = load_fixture("mtx_small.json")
+    hg = HostGraph(np.array(fx["row_offsets"], np.int32), np.array(fx["column_indices"], np.int32), directed=True)
+    t = hg.transpose()
+    want = oracle.bfs_pred(t.row_offsets, t.column_indices, np.array(ex["bfs"]["0"], np.int32))
+    assert [int(x) for x in got["bfs_pred"]] == want.tolist()

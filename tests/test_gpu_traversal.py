@@ -1,6 +1,8 @@
 """GPU parity of the CUDA GAS path (through the C ABI) against the golden
 vectors of the reference CPU code and the oracle: BFS depths, SSSP distances and
 CC labels bit-exact; the reference PageRank program within FP32 tolerance."""
+import ctypes as C
+
 import numpy as np
 import pytest
 
@@ -170,3 +172,31 @@ def test_repeated_runs_reuse_workspace():
     for _ in range(5):
         assert np.array_equal(g.bfs(s)[0], ref_b)
         assert np.array_equal(g.sssp(s)[0], ref_s)
+
+
+@pytest.mark.parametrize("kind", ["rmat_sym", "rmat_directed", "road"])
+def test_bfs_pred_matches_oracle(kind):
+    # mg_bfs_pred against the oracle's restatement of pred_extract, bit-exact, with
+    # depths equal to mg_bfs and host and device outputs agreeing.
+    import torch
+
+    if kind == "rmat_sym":
+        hg = HostGraph.rmat(14, 16, seed=4)
+    elif kind == "rmat_directed":
+        hg = HostGraph.rmat(13, 8, seed=5, symmetrize=False)
+    else:
+        hg = HostGraph.road_grid(120, 0.02, 0.005, seed=6)
+    g = Graph(hg)
+    t = hg.transpose() if hg.directed else hg
+    for s in (hg.max_degree_vertex(), 1):
+        d, p, st = g.bfs_pred(s)
+        ref_d = oracle.bfs(hg.row_offsets, hg.column_indices, s)
+        assert np.array_equal(d, ref_d)
+        assert np.array_equal(p, oracle.bfs_pred(t.row_offsets, t.column_indices, ref_d))
+        dd = torch.empty(hg.nodes, dtype=torch.int32, device="cuda")
+        pd = torch.empty(hg.nodes, dtype=torch.int32, device="cuda")
+        o = _lib.default_options(outputs_on_device=1)
+        _lib.check(_lib.lib.mg_bfs_pred(g.handle, int(s), dd.data_ptr(), pd.data_ptr(), None, C.byref(o)),
+                   "mg_bfs_pred")
+        assert np.array_equal(pd.cpu().numpy(), p) and np.array_equal(dd.cpu().numpy(), d)
+    g.close()

@@ -96,3 +96,31 @@ def test_pr_gas_restatement_close_to_reference_cpupr():
     ref = oracle.ref_pr(g.row_offsets, g.column_indices, t.row_offsets, t.column_indices)
     rel = np.linalg.norm(mine - ref) / np.linalg.norm(ref)
     assert rel < 0.1  # the reference's own check (PageRank.cu:305-315, tol default 0.1)
+
+
+def test_bfs_pred_known_answer_directed():
+    # 0->1, 0->2, 1->3, 2->3, 3->4, 5->0. From 0: depths [0, 1, 1, 2, 3, -1]. pred_extract's
+    # rule takes the largest in-neighbour one level up; the root's unreached in-neighbour 5
+    # (depth -1) also satisfies depth[v] - depth[u] == 1, as in the reference's arithmetic.
+    ro = np.array([0, 2, 3, 4, 5, 5, 6], np.int32)
+    col = np.array([1, 2, 3, 3, 4, 0], np.int32)
+    g = HostGraph(ro, col, directed=True)
+    t = g.transpose()
+    d = oracle.bfs(ro, col, 0)
+    assert d.tolist() == [0, 1, 1, 2, 3, -1]
+    assert oracle.bfs_pred(t.row_offsets, t.column_indices, d).tolist() == [5, 0, 0, 2, 3, -1]
+
+
+@pytest.mark.parametrize("seed", [1, 2])
+def test_bfs_pred_is_a_bfs_tree(seed):
+    # Graph500-style checks: every reached non-root vertex has a predecessor that is an
+    # in-neighbour one level up, and it is the largest such in-neighbour.
+    g = HostGraph.rmat(12, 8, seed=seed)
+    src = g.max_degree_vertex()
+    d = oracle.bfs(g.row_offsets, g.column_indices, src)
+    p = oracle.bfs_pred(g.row_offsets, g.column_indices, d)
+    assert p[src] == -1 and (p[d < 0] == -1).all()
+    for v in np.flatnonzero(d > 0):
+        nb = g.column_indices[g.row_offsets[v]:g.row_offsets[v + 1]]
+        up = nb[d[nb] == d[v] - 1]
+        assert len(up) > 0 and p[v] == up.max()
