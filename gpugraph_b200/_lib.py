@@ -109,6 +109,7 @@ SIGNATURES = {
     "mg_build_road_grid": (C.c_int, [C.c_int32, C.c_double, C.c_double, C.c_uint64, CSRP]),
     "mg_build_weights": (C.c_int, [CSRP, C.c_uint32, C.c_uint32, C.c_uint64]),
     "mg_read_market": (C.c_int, [C.c_char_p, C.c_int32, CSRP]),
+    "mg_read_csv": (C.c_int, [C.c_char_p, C.c_int32, C.c_int32, CSRP]),
     "mg_host_csr_transpose": (C.c_int, [CSRP, CSRP]),
     "mg_host_csr_free": (None, [CSRP]),
 }

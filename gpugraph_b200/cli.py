@@ -24,7 +24,7 @@ from . import Graph, HostGraph
 from ._lib import MG_DIR_AUTO, MG_DIR_PULL, MG_DIR_PUSH
 
 KNOWN = {"src", "directed", "iter_num", "threshold", "tol", "direction", "alpha", "beta", "alpha_multi",
-         "use_cuda_graph", "ctas_per_sm", "run_CPU", "weights"}
+         "use_cuda_graph", "ctas_per_sm", "run_CPU", "weights", "csv_format"}
 DIRS = {"auto": MG_DIR_AUTO, "push": MG_DIR_PUSH, "pull": MG_DIR_PULL}
 
 
@@ -82,7 +82,11 @@ def main(argv=None) -> int:
 
     if args.graph:
         directed = params.get("directed", "1") != "0"
-        hg = HostGraph.read_market(args.graph, undirected=not directed)
+        if args.graph.endswith(".csv"):
+            # the reference's BFS driver reads CSV graphs as undirected adjacency rows (bfs.cu:519-520)
+            hg = HostGraph.read_csv(args.graph, params.get("csv_format", "adjacency"), undirected=not directed)
+        else:
+            hg = HostGraph.read_market(args.graph, undirected=not directed)
     elif args.rmat:
         hg = HostGraph.rmat(args.rmat, args.ef, seed=args.seed, symmetrize=not args.directed)
     elif args.grid:

@@ -8,6 +8,7 @@
 #include <cmath>
 #include <cstdio>
 #include <cstdlib>
+#include <climits>
 #include <cstring>
 #include <string>
 #include <thread>
@@ -328,6 +329,94 @@ int mg_read_market(const char *path, int32_t undirected, mg_host_csr *out) {
   if (nodes < 0) return set_error(MG_ERR_IO, "no graph found");
   if ((int64_t)coo.size() != (undirected ? 2 * declared : declared))
     return set_error(MG_ERR_IO, "edge count does not match the size line");
+  std::stable_sort(coo.begin(), coo.end(), [](const Tup &x, const Tup &y) {
+    return x.row < y.row || (x.row == y.row && x.col < y.col);
+  });
+  if (!alloc_csr(out, nodes, (int64_t)coo.size(), true)) return set_error(MG_ERR_OOM, "host allocation failed");
+  std::fill(out->row_offsets, out->row_offsets + nodes + 1, 0);
+  for (auto &t : coo) out->row_offsets[t.row + 1]++;
+  for (int64_t v = 0; v < nodes; ++v) out->row_offsets[v + 1] += out->row_offsets[v];
+  for (size_t i = 0; i < coo.size(); ++i) {
+    out->column_indices[i] = coo[i].col;
+    out->edge_values[i] = coo[i].val;
+  }
+  out->directed = undirected ? 0 : 1;
+  return MG_OK;
+}
+
+// CSV graphs as csv_graph_reader reads them (GASengine/csv_graph_reader.cuh):
+// format 0 (read(), :79-137) has one row per source, "src,dst:val,dst:val,...";
+// format 1 (read2(), :147-205) one row per edge, "src,dst,val". Every id that
+// appears (a lone "src" row included) becomes a vertex, numbered by sorted id
+// (:98-111); `undirected` appends the reversed edges (:127-135); the CSR is
+// ordered by (row, col) keeping duplicates (b40c CsrGraph::FromCoo with
+// DimacsTupleCompare). A format-0 cell without ':' gives its own number as the
+// value (the reference's substr(npos + 1) is the whole cell). Empty lines are
+// skipped.
+int mg_read_csv(const char *path, int32_t format, int32_t undirected, mg_host_csr *out) {
+  if (!path || !out) return set_error(MG_ERR_ARG, "path/out is NULL");
+  if (format != 0 && format != 1) return set_error(MG_ERR_ARG, "format must be 0 (adjacency rows) or 1 (edge rows)");
+  memset(out, 0, sizeof(*out));
+  FILE *f = fopen(path, "r");
+  if (!f) return set_error(MG_ERR_IO, std::string("cannot open ") + path);
+  struct Tup {
+    int32_t row, col, val;
+  };
+  std::vector<Tup> coo;
+  std::vector<int32_t> ids;
+  std::string line;
+  std::vector<std::string> cells;
+  char buf[1 << 16];
+  bool bad = false;
+  while (!bad && fgets(buf, sizeof(buf), f)) {
+    line.assign(buf);
+    // a line longer than the buffer continues in the next reads
+    while (!line.empty() && line.back() != '\n' && fgets(buf, sizeof(buf), f)) line.append(buf);
+    while (!line.empty() && (line.back() == '\n' || line.back() == '\r')) line.pop_back();
+    if (line.empty()) continue;
+    cells.clear();
+    size_t b = 0;
+    for (;;) {
+      const size_t e = line.find(',', b);
+      cells.push_back(line.substr(b, e == std::string::npos ? std::string::npos : e - b));
+      if (e == std::string::npos) break;
+      b = e + 1;
+    }
+    const int32_t src = (int32_t)atoi(cells[0].c_str());
+    ids.push_back(src);
+    if (format == 1) {
+      if (cells.size() < 3) {
+        bad = true;
+        break;
+      }
+      const int32_t dst = (int32_t)atoi(cells[1].c_str());
+      ids.push_back(dst);
+      coo.push_back({src, dst, (int32_t)atoi(cells[2].c_str())});
+      continue;
+    }
+    for (size_t i = 1; i < cells.size(); ++i) {
+      const size_t pos = cells[i].find(':');
+      const int32_t dst = (int32_t)atoi(cells[i].substr(0, pos).c_str());
+      const int32_t val = (int32_t)atoi(pos == std::string::npos ? cells[i].c_str() : cells[i].c_str() + pos + 1);
+      ids.push_back(dst);
+      coo.push_back({src, dst, val});
+    }
+  }
+  fclose(f);
+  if (bad) return set_error(MG_ERR_IO, "an edge row needs src,dst,val");
+  std::sort(ids.begin(), ids.end());
+  ids.erase(std::unique(ids.begin(), ids.end()), ids.end());
+  const int64_t nodes = (int64_t)ids.size();
+  auto dense = [&](int32_t id) { return (int32_t)(std::lower_bound(ids.begin(), ids.end(), id) - ids.begin()); };
+  for (auto &t : coo) {
+    t.row = dense(t.row);
+    t.col = dense(t.col);
+  }
+  if (undirected) {
+    const size_t m = coo.size();
+    for (size_t i = 0; i < m; ++i) coo.push_back({coo[i].col, coo[i].row, coo[i].val});
+  }
+  if ((int64_t)coo.size() > INT32_MAX) return set_error(MG_ERR_OVERFLOW, "more than 2^31-1 edges");
   std::stable_sort(coo.begin(), coo.end(), [](const Tup &x, const Tup &y) {
     return x.row < y.row || (x.row == y.row && x.col < y.col);
   });

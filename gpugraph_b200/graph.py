@@ -83,6 +83,15 @@ class HostGraph:
         check(lib.mg_read_market(str(path).encode(), int(undirected), C.byref(h)), "mg_read_market")
         return HostGraph._from_c(h)
 
+    @staticmethod
+    def read_csv(path: str, fmt: str = "adjacency", undirected: bool = True) -> "HostGraph":
+        """CSV graph as the reference's csv_graph_reader reads it: fmt "adjacency" for rows
+        "src,dst:val,...", "edges" for rows "src,dst,val"; ids renumbered in sorted order."""
+        h = _lib.HostCsr()
+        f = {"adjacency": 0, "edges": 1}[fmt]
+        check(lib.mg_read_csv(str(path).encode(), f, int(undirected), C.byref(h)), "mg_read_csv")
+        return HostGraph._from_c(h)
+
     def with_weights(self, lo: int, hi: int, seed: int = 1) -> "HostGraph":
         """Symmetric uint32 weights w(u,v)=w(v,u) in [lo, hi] (a copy of self)."""
         g = HostGraph(self.row_offsets.copy(), self.column_indices.copy(), None, self.directed, self.graph_offsets)

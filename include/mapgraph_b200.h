@@ -251,6 +251,10 @@ int mg_build_weights(mg_host_csr *csr, uint32_t lo, uint32_t hi, uint64_t seed);
  * and duplicates kept. A "pattern" file gets value 1 on every edge. */
 int mg_read_market(const char *path, int32_t undirected, mg_host_csr *out);
 /* Transpose (CSC) of a host CSR: column offsets and row indices, stable by row. */
+/* CSV graph (GASengine/csv_graph_reader.cuh): format 0 = rows "src,dst:val,...",
+ * format 1 = rows "src,dst,val"; ids renumbered densely in sorted order;
+ * undirected != 0 adds the reversed edges. Edge values are int32. */
+int mg_read_csv(const char *path, int32_t format, int32_t undirected, mg_host_csr *out);
 int mg_host_csr_transpose(const mg_host_csr *in, mg_host_csr *out);
 void mg_host_csr_free(mg_host_csr *csr);
 

@@ -11,7 +11,7 @@ import pytest
 from conftest import fixture_names, host_graph_from_fixture, load_fixture
 
 import gpugraph_b200 as gg
-from gpugraph_b200 import _lib
+from gpugraph_b200 import HostGraph, MapGraphError, _lib
 
 HEADER = Path(__file__).resolve().parents[1] / "include" / "mapgraph_b200.h"
 
@@ -164,3 +164,36 @@ def test_null_graph_arguments():
 def test_kernel_launch_counter_resets():
     _lib.lib.mg_kernel_launches(1)
     assert _lib.lib.mg_kernel_launches(0) == 0
+
+
+def test_csv_reader_adjacency_rows(tmp_path):
+    # csv_graph_reader::read: "src,dst:val,..." rows; ids 10, 20, 30, 40 -> 0..3 in sorted
+    # order; a lone "40" row still makes a vertex; a cell without ':' takes its own
+    # number as the value; undirected appends the reversed edges; CSR sorted by (row, col).
+    p = tmp_path / "g.csv"
+    p.write_text("20,10:5,30:7\n10,30:2\n\n40\n30,20\n")
+    g = HostGraph.read_csv(str(p), "adjacency", undirected=False)
+    assert g.nodes == 4 and g.directed
+    assert g.row_offsets.tolist() == [0, 1, 3, 4, 4]
+    assert g.column_indices.tolist() == [2, 0, 2, 1]
+    assert g.edge_values.tolist() == [2, 5, 7, 20]
+    u = HostGraph.read_csv(str(p), "adjacency", undirected=True)
+    assert not u.directed and u.edges == 8
+    assert u.row_offsets.tolist() == [0, 2, 5, 8, 8]
+    assert u.column_indices.tolist() == [1, 2, 0, 2, 2, 0, 1, 1]
+
+
+def test_csv_reader_edge_rows_and_errors(tmp_path):
+    # csv_graph_reader::read2: "src,dst,val" rows, duplicates kept
+    p = tmp_path / "e.csv"
+    p.write_text("7,3,1\n3,9,4\n7,3,2\n")
+    g = HostGraph.read_csv(str(p), "edges", undirected=False)
+    assert g.nodes == 3
+    assert g.row_offsets.tolist() == [0, 1, 3, 3]
+    assert g.column_indices.tolist() == [2, 0, 0] and g.edge_values.tolist() == [4, 1, 2]
+    bad = tmp_path / "bad.csv"
+    bad.write_text("1,2\n")
+    with pytest.raises(MapGraphError):
+        HostGraph.read_csv(str(bad), "edges")
+    with pytest.raises(MapGraphError):
+        HostGraph.read_csv(str(tmp_path / "missing.csv"))
