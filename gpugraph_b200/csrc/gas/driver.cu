@@ -9,52 +9,7 @@
 
 namespace mg {
 
-__global__ void k_level_end(Ctl *ctl, cudaGraphConditionalHandle h, int use_handle) {
-  if (threadIdx.x != 0) return;
-  if (ctl->active) {
-    ctl->level += 1;
-    ctl->push_levels += 1;
-    ctl->frontier_size = ctl->next_size;
-    ctl->next_size = 0;
-    ctl->edge_total = 0;
-    ctl->exp_tiles = 0;
-    ctl->next_edges = 0;
-    ctl->epoch += 4;
-    for (int i = 0; i < 4; ++i) ctl->tile_ctr[i] = 0;
-    ctl->active = (ctl->frontier_size > 0 && ctl->level < ctl->max_iter && ctl->error == 0) ? 1u : 0u;
-  }
-  if (use_handle) cudaGraphSetConditional(h, ctl->active);
-}
-
-__global__ void k_fill_i32(int32_t *p, int32_t v, int64_t n) {
-  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
-    p[i] = v;
-}
-
-__global__ void k_sequence_i32(int32_t *p, int64_t n) {
-  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
-    p[i] = (int32_t)i;
-}
-
-__global__ void k_ctl_init(Ctl *ctl, uint32_t frontier_size, uint32_t max_iter, unsigned long long spin_limit,
-                           uint32_t mode, uint32_t flags) {
-  if (threadIdx.x != 0) return;
-  // The epoch keeps growing across runs so stale look-back words never match;
-  // the host zeroes the status words and the control block before the 30-bit
-  // field could wrap (see prepare_run).
-  const uint32_t epoch = ctl->epoch + 4;
-  Ctl c;
-  memset(&c, 0, sizeof(c));
-  c.epoch = epoch;
-  c.frontier_size = frontier_size;
-  c.max_iter = max_iter;
-  c.spin_limit = spin_limit;
-  c.mode = mode;
-  c.next_mode = mode;
-  c.active = (frontier_size > 0 && max_iter > 0) ? 1u : 0u;
-  c.ordered = flags & 1u;
-  *ctl = c;
-}
+constexpr size_t kMaxCachedLoops = 64;
 
 int read_ctl(mg_graph *g, cudaStream_t s, Ctl *out) {
   cudaError_t e = cudaMemcpyAsync(g->host_ctl, g->ws.ctl, sizeof(Ctl), cudaMemcpyDeviceToHost, s);
@@ -172,6 +127,15 @@ int run_level_loop(mg_graph *g, cudaStream_t s, const std::string &key, int kern
   bool graphed = false;
   if (use_graph && !prof_on()) {
     auto it = g->loops.find(key);
+    if (it == g->loops.end() && g->loops.size() >= kMaxCachedLoops) {
+      // bound the cache (keys include argument hashes): drop every cached
+      // graph; the ones still in use are rebuilt on their next run
+      for (auto &kv : g->loops) {
+        if (kv.second.exec) cudaGraphExecDestroy(kv.second.exec);
+        if (kv.second.graph) cudaGraphDestroy(kv.second.graph);
+      }
+      g->loops.clear();
+    }
     if (it == g->loops.end()) {
       LoopCache lc;
       lc.kernels_per_level = kernels_per_level;

@@ -346,7 +346,6 @@ __global__ void __launch_bounds__(kNT) k_expand(GasArgs<P> a) {
   for (;;) {
     const uint32_t tile = next_tile(&ctl->tile_ctr[1], &s_tile);
     if (tile >= ntiles || s_fail) break;
-    const unsigned long long d0 = (unsigned long long)tile * NV;
     int cnt;
     if (!decode_tile<VT>(tile, ntiles, n, items, a.part, a.scan, F, ro, s_v, s_base, s_rs, s_own, s_warpmax, &cnt,
                          [&](int j, int v) { s_ch[j] = (uint8_t)ev(v, (char)a.changed[v], a.vl, a.el); })) {
@@ -463,17 +462,61 @@ __global__ void __launch_bounds__(kNT) k_expand(GasArgs<P> a) {
   }
 }
 
+// The small kernels every level loop launches are defined here with internal
+// linkage, so each translation unit that launches them (the library's and a
+// separately built Program's alike) registers and launches its own copy.
+
 // ---------------------------------------------------------------- level end -
 // Advances the level and decides whether the loop continues; inside a CUDA
 // graph it drives the WHILE node's condition.
-__global__ void k_level_end(Ctl *ctl, cudaGraphConditionalHandle h, int use_handle);
+static __global__ void k_level_end(Ctl *ctl, cudaGraphConditionalHandle h, int use_handle) {
+  if (threadIdx.x != 0) return;
+  if (ctl->active) {
+    ctl->level += 1;
+    ctl->push_levels += 1;
+    ctl->frontier_size = ctl->next_size;
+    ctl->next_size = 0;
+    ctl->edge_total = 0;
+    ctl->exp_tiles = 0;
+    ctl->next_edges = 0;
+    ctl->epoch += 4;
+    for (int i = 0; i < 4; ++i) ctl->tile_ctr[i] = 0;
+    ctl->active = (ctl->frontier_size > 0 && ctl->level < ctl->max_iter && ctl->error == 0) ? 1u : 0u;
+  }
+  if (use_handle) cudaGraphSetConditional(h, ctl->active);
+}
 
-// --------------------------------------------------------------- utilities --
-__global__ void k_fill_i32(int32_t *p, int32_t v, int64_t n);
-__global__ void k_sequence_i32(int32_t *p, int64_t n);
+static __global__ void k_fill_i32(int32_t *p, int32_t v, int64_t n) {
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+    p[i] = v;
+}
+
+static __global__ void k_sequence_i32(int32_t *p, int64_t n) {
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+    p[i] = (int32_t)i;
+}
+
 // flags: bit 0 = ordered frontier compaction (mg_options.ordered_frontier)
-__global__ void k_ctl_init(Ctl *ctl, uint32_t frontier_size, uint32_t max_iter, unsigned long long spin_limit,
-                           uint32_t mode, uint32_t flags);
+static __global__ void k_ctl_init(Ctl *ctl, uint32_t frontier_size, uint32_t max_iter, unsigned long long spin_limit,
+                           uint32_t mode, uint32_t flags) {
+  if (threadIdx.x != 0) return;
+  // The epoch keeps growing across runs so stale look-back words never match;
+  // the host zeroes the status words and the control block before the 30-bit
+  // field could wrap (see prepare_run).
+  const uint32_t epoch = ctl->epoch + 4;
+  Ctl c;
+  memset(&c, 0, sizeof(c));
+  c.epoch = epoch;
+  c.frontier_size = frontier_size;
+  c.max_iter = max_iter;
+  c.spin_limit = spin_limit;
+  c.mode = mode;
+  c.next_mode = mode;
+  c.active = (frontier_size > 0 && max_iter > 0) ? 1u : 0u;
+  c.ordered = flags & 1u;
+  *ctl = c;
+}
+
 inline uint32_t ctl_flags(const mg_options *o) { return (o && o->ordered_frontier) ? 1u : 0u; }
 
 }  // namespace mg

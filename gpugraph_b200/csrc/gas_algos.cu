@@ -13,82 +13,13 @@
 #include "gas/driver.cuh"
 #include "gas/engine.cuh"
 #include "gas/programs.cuh"
+#include "gas/run_gas.cuh"
 
 namespace mg {
-
-constexpr int kVTS = 4;
-constexpr int kVT = 8;
-
-template <class P>
-GasArgs<P> base_args(mg_graph *g) {
-  Workspace &w = g->ws;
-  GasArgs<P> a;
-  a.g = g->csr;
-  a.queue0 = w.queue[0];
-  a.queue1 = w.queue[1];
-  a.scan = w.scan;
-  a.part = w.part;
-  a.status = w.status;
-  a.bm0 = w.bm[0];
-  a.bm1 = w.bm[1];
-  a.changed = w.changed;
-  a.gather_tmp = reinterpret_cast<typename P::GatherType *>(w.gather_tmp);
-  a.gather_res = reinterpret_cast<typename P::GatherType *>(w.vbuf[1]);
-  a.ctl = w.ctl;
-  a.expand_in = (P::expandOverEdges() == EXPAND_IN_EDGES) ? 1 : 0;
-  a.gather_dir = (int32_t)P::gatherOverEdges();
-  return a;
-}
 
 __global__ void k_fill_u32(uint32_t *p, uint32_t v, int64_t n) {
   for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
     p[i] = v;
-}
-
-// Generic level loop for a Program: gather -> apply -> post_apply -> scan ->
-// expand/contract -> level end. n0 = initial frontier size (already in queue 0).
-template <class P>
-int run_gas(mg_graph *g, const GasArgs<P> &a, uint32_t n0, const mg_options *o, const char *name, LoopResult *res) {
-  cudaStream_t s = run_stream(g, o);
-  const int grid = persistent_grid(g, o, 4);
-  // Every level of a traversal settles at least one vertex, so V + 2 levels bound
-  // the device loop even if a Program never empties its frontier.
-  const uint32_t max_iter = (uint32_t)std::min<int64_t>(o->iter_num > 0 ? o->iter_num : 0, g->nodes + 2);
-  cudaError_t e = cudaMemsetAsync(g->ws.bm[0], 0, g->ws.words * 4, s);
-  if (e == cudaSuccess) e = cudaMemsetAsync(g->ws.bm[1], 0, g->ws.words * 4, s);
-  if (e == cudaSuccess) e = cudaMemsetAsync(g->ws.changed, 0, (size_t)g->nodes, s);
-  int st = cuda_status(e, "gas init");
-  if (st != MG_OK) return st;
-  k_ctl_init<<<1, 32, 0, s>>>(a.ctl, n0, max_iter, (unsigned long long)o->spin_limit, MODE_QUEUE, ctl_flags(o));
-  count_launch();
-  const bool gather = P::gatherOverEdges() != NO_GATHER_EDGES;
-  const bool apply = P::applyOverEdges() != NO_APPLY_VERTICES;
-  const bool post = P::postApplyOverEdges() != NO_POST_APPLY_VERTICES;
-  const int apply_all = P::applyOverEdges() == APPLY_ALL;
-  const int post_all = P::postApplyOverEdges() == POST_APPLY_ALL;
-  const int kpl = 3 + (gather ? 1 : 0) + (apply ? 1 : 0) + (post ? 1 : 0);
-  // expand tile: 1024 or 2048 items (mg_options.tile_items; 0 = 2048)
-  const bool small_tiles = o->tile_items > 0 && o->tile_items <= 1024;
-  LevelBody body = [=](cudaStream_t ss, cudaGraphConditionalHandle h, int use_h) {
-    if (gather) MG_LAUNCH(KID_GATHER, ss, k_gather<P><<<grid, kNT, 0, ss>>>(a));
-    if (apply) MG_LAUNCH(KID_APPLY, ss, k_apply<P><<<grid, kNT, 0, ss>>>(a, apply_all, gather ? 1 : 0));
-    if (post) MG_LAUNCH(KID_APPLY, ss, k_post_apply<P><<<grid, kNT, 0, ss>>>(a, post_all));
-    if (small_tiles) {
-      MG_LAUNCH(KID_SCAN, ss, (k_frontier_scan<P, kVTS, 4><<<grid, kNT, 0, ss>>>(a)));
-      MG_LAUNCH(KID_EXPAND, ss, (k_expand<P, 4><<<grid, kNT, 0, ss>>>(a)));
-    } else {
-      MG_LAUNCH(KID_SCAN, ss, (k_frontier_scan<P, kVTS, kVT><<<grid, kNT, 0, ss>>>(a)));
-      MG_LAUNCH(KID_EXPAND, ss, (k_expand<P, kVT><<<grid, kNT, 0, ss>>>(a)));
-    }
-    MG_LAUNCH(KID_OTHER, ss, k_level_end<<<1, 32, 0, ss>>>(a.ctl, h, use_h));
-  };
-  st = run_level_loop(g, s, std::string(name) + "/" + std::to_string(grid) + (small_tiles ? "/t1024" : "/t2048"),
-                      kpl, body, o->use_cuda_graph != 0, res);
-  if (st != MG_OK) return st;
-  finish_run(g, res->ctl.level);
-  if (res->ctl.error)
-    return set_error(res->ctl.error, std::string(name) + ": device reported " + mg_status_string(res->ctl.error));
-  return MG_OK;
 }
 
 static void fill_stats(mg_stats *stats, const LoopResult &res) {
