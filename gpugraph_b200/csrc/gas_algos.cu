@@ -17,6 +17,8 @@
 
 namespace mg {
 
+int cc_union_find(mg_graph *g, int32_t *labels, mg_stats *stats, const mg_options *o);  // cc.cu
+
 __global__ void k_fill_u32(uint32_t *p, uint32_t v, int64_t n) {
   for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
     p[i] = v;
@@ -88,8 +90,11 @@ int mg_sssp(mg_graph *g, int32_t src, int32_t *dists, mg_stats *stats, const mg_
 int mg_cc(mg_graph *g, int32_t *labels, mg_stats *stats, const mg_options *opts) {
   clear_error();
   if (!g) return set_error(MG_ERR_ARG, "graph is NULL");
+  if (!labels) return set_error(MG_ERR_ARG, "labels is NULL");
   mg_options d;
   const mg_options *o = opts_or_default(opts, &d);
+  // symmetric graph: the same labels in one union-find pass (cc.cu)
+  if (!g->directed) return cc_union_find(g, labels, stats, o);
   cudaStream_t s = run_stream(g, o);
   int st = prepare_run(g, s);
   if (st != MG_OK) return st;
