@@ -33,6 +33,11 @@ namespace mg {
 typedef unsigned long long u64;
 constexpr int kMVTS = 4;
 constexpr int kMVT = 8;
+// Batched SSSP relaxes four edges per warp step (each 512 bytes of distance
+// rows), so its expand tiles are the smallest the workspace allows (1024
+// items): more CTAs share a level's edges.
+constexpr int kMSVT = 4;
+constexpr int kMssSparse = 24; // active sources per edge up to which a lane relaxes a whole edge alone
 
 // Push step of the batched BFS as a GAS Program: expand_edge emits the
 // sources that reach the neighbour for the first time, contract ORs them into
@@ -563,62 +568,42 @@ __global__ void __launch_bounds__(kNT) k_mss_expand(MultiArgs a, const uint32_t 
       __syncthreads();
       break;
     }
-    // Four edges per warp step: the 8 lanes of group g relax edge k0+4s+g, lane
-    // `sub` owning sources 8*sub .. 8*sub+7, whose distances it reads with two
-    // 16-byte loads from each 256-byte row.
+    // The warp takes its items 32 at a time; lane i loads item k+i's edge (tail,
+    // head, weight, tail's source mask), the next batch while the current one
+    // is relaxed. If every edge of the batch carries at most kMssSparse active
+    // sources, each lane relaxes its own edge source by source (scalar loads
+    // from the two 256-byte rows); otherwise the batch goes four edges per
+    // step, the 8 lanes of group g owning sources 8*sub .. 8*sub+7 of edge
+    // 4q+g, read with two 16-byte loads from each row.
     const int k0 = warp * PER_WARP;
     const int k1 = min(cnt, k0 + PER_WARP);
     const int grp = lane >> 3, sub = lane & 7;
-    for (int kb = k0; kb < k1; kb += 4) {
-      const int k = kb + grp;
-      int v = -1;
-      uint32_t imp = 0;
-      if (k < k1) {
-        const int j = s_own[k];
-        const int el = k - s_base[j] - 1;
-        if (el >= 0) {
-          const int u = s_v[j];
-          const int eid = s_rs[j] + el;
-          if ((unsigned)eid < (unsigned)a.g.E) {
-            v = col[eid];
-            const int w = wgt[eid];
-            const u64 am = Fc[u];
-            const uint32_t bits = (uint32_t)(am >> (8 * sub)) & 0xffu;
-            // column, weight, source mask; both distances of every active source
-            if (sub == 0) my_bytes += 16 + 8ull * (unsigned long long)__popcll(am);
-            if (bits) {
-              const int4 *pu = reinterpret_cast<const int4 *>(a.out + (int64_t)u * 64 + 8 * sub);
-              int32_t *dvp = a.out + (int64_t)v * 64 + 8 * sub;
-              const int4 *pv = reinterpret_cast<const int4 *>(dvp);
-              const int4 u0 = pu[0], u1 = pu[1], v0 = pv[0], v1 = pv[1];
-              const int du[8] = {u0.x, u0.y, u0.z, u0.w, u1.x, u1.y, u1.z, u1.w};
-              const int dv[8] = {v0.x, v0.y, v0.z, v0.w, v1.x, v1.y, v1.z, v1.w};
-#pragma unroll
-              for (int t = 0; t < 8; ++t) {
-                if ((bits >> t) & 1u) {
-                  const int c = du[t] + w;
-                  if (c < dv[t] && atomicMin(&dvp[t], c) > c) imp |= 1u << t;
-                }
-              }
-            }
-          } else {
-            raise_error(ctl, MG_ERR_OVERFLOW);
-          }
-        }
+    auto fetch = [&](int k, int &u, int &v, int &w, u64 &am) {
+      u = -1;
+      if (k >= k1) return;
+      const int j = s_own[k];
+      const int el = k - s_base[j] - 1;
+      if (el < 0) return;
+      const int eid = s_rs[j] + el;
+      if ((unsigned)eid >= (unsigned)a.g.E) {
+        raise_error(ctl, MG_ERR_OVERFLOW);
+        return;
       }
-      // improved sources of the group's edge: OR of the 8 lanes' byte masks
-      u64 mask = (u64)imp << (8 * sub);
-      mask |= __shfl_xor_sync(0xffffffffu, mask, 1);
-      mask |= __shfl_xor_sync(0xffffffffu, mask, 2);
-      mask |= __shfl_xor_sync(0xffffffffu, mask, 4);
+      u = s_v[j];
+      v = col[eid];
+      w = wgt[eid];
+      am = Fc[u];
+    };
+    // next-level mask, dedup bit and queue slot for the vertices that improved
+    auto enqueue = [&](bool has, int v, u64 mask) {
       bool enq = false;
-      if (sub == 0 && mask) {
+      if (has) {
         my_bytes += 8 + 4ull * (unsigned long long)__popcll(mask);
         atomicOr(&Fn[v], mask);
         const uint32_t bit = 1u << (v & 31);
         enq = !(ld_volatile(&dedup[v >> 5]) & bit) && !(atomicOr(&dedup[v >> 5], bit) & bit);
       }
-      // one queue reservation per warp step for its (up to four) new vertices
+      // one queue reservation per warp step
       const uint32_t eb = __ballot_sync(0xffffffffu, enq);
       if (eb) {
         uint32_t base = 0;
@@ -629,6 +614,59 @@ __global__ void __launch_bounds__(kNT) k_mss_expand(MultiArgs a, const uint32_t 
           if (pos < (uint32_t)V) Qn[pos] = v;
           else raise_error(ctl, MG_ERR_OVERFLOW);
         }
+      }
+    };
+    int nu = -1, nv = 0, nw = 0;
+    u64 nam = 0;
+    fetch(k0 + lane, nu, nv, nw, nam);
+    for (int kb = k0; kb < k1; kb += 32) {
+      const int bu = nu, bv = nv, bw = nw;
+      const u64 bam = nam;
+      fetch(kb + 32 + lane, nu, nv, nw, nam);
+      if (bu >= 0) my_bytes += 16 + 8ull * (unsigned long long)__popcll(bam);
+      if (__all_sync(0xffffffffu, bu < 0 || __popcll(bam) <= kMssSparse)) {
+        u64 imp = 0;
+        if (bu >= 0) {
+          const int32_t *du = a.out + (int64_t)bu * 64;
+          int32_t *dv = a.out + (int64_t)bv * 64;
+          for (u64 m = bam; m; m &= m - 1) {
+            const int t = __ffsll((long long)m) - 1;
+            const int c = du[t] + bw;
+            if (c < dv[t] && atomicMin(&dv[t], c) > c) imp |= 1ull << t;
+          }
+        }
+        enqueue(imp != 0, bv, imp);
+        continue;
+      }
+#pragma unroll 1
+      for (int q = 0; q < 8; ++q) {
+        const int src = 4 * q + grp;
+        const int u = __shfl_sync(0xffffffffu, bu, src), v = __shfl_sync(0xffffffffu, bv, src);
+        const int w = __shfl_sync(0xffffffffu, bw, src);
+        const u64 am = __shfl_sync(0xffffffffu, bam, src);
+        uint32_t imp = 0;
+        const uint32_t bits = u >= 0 ? (uint32_t)(am >> (8 * sub)) & 0xffu : 0u;
+        if (bits) {
+          const int4 *pu = reinterpret_cast<const int4 *>(a.out + (int64_t)u * 64 + 8 * sub);
+          int32_t *dvp = a.out + (int64_t)v * 64 + 8 * sub;
+          const int4 *pv = reinterpret_cast<const int4 *>(dvp);
+          const int4 u0 = pu[0], u1 = pu[1], v0 = pv[0], v1 = pv[1];
+          const int du[8] = {u0.x, u0.y, u0.z, u0.w, u1.x, u1.y, u1.z, u1.w};
+          const int dv[8] = {v0.x, v0.y, v0.z, v0.w, v1.x, v1.y, v1.z, v1.w};
+#pragma unroll
+          for (int t = 0; t < 8; ++t) {
+            if ((bits >> t) & 1u) {
+              const int c = du[t] + w;
+              if (c < dv[t] && atomicMin(&dvp[t], c) > c) imp |= 1u << t;
+            }
+          }
+        }
+        // improved sources of the group's edge: OR of the 8 lanes' byte masks
+        u64 mask = (u64)imp << (8 * sub);
+        mask |= __shfl_xor_sync(0xffffffffu, mask, 1);
+        mask |= __shfl_xor_sync(0xffffffffu, mask, 2);
+        mask |= __shfl_xor_sync(0xffffffffu, mask, 4);
+        enqueue(sub == 0 && mask != 0, v, mask);
       }
     }
   }
@@ -879,8 +917,8 @@ int mg_sssp_multi(mg_graph *g, const int32_t *srcs, int32_t nsrc, int32_t *dists
   int32_t *part = g->ws.part;
   LevelBody body = [=](cudaStream_t ss, cudaGraphConditionalHandle h, int use_h) {
     MG_LAUNCH(KID_MS_APPLY, ss, k_mss_clear<<<grid, kNT, 0, ss>>>(a));
-    MG_LAUNCH(KID_SCAN, ss, (k_frontier_scan<mssp_scan, kMVTS, kMVT><<<grid, kNT, 0, ss>>>(ga)));
-    MG_LAUNCH(KID_MSS_EXPAND, ss, k_mss_expand<kMVT><<<grid, kNT, 0, ss>>>(a, scan, part));
+    MG_LAUNCH(KID_SCAN, ss, (k_frontier_scan<mssp_scan, kMVTS, kMSVT><<<grid, kNT, 0, ss>>>(ga)));
+    MG_LAUNCH(KID_MSS_EXPAND, ss, k_mss_expand<kMSVT><<<grid, kNT, 0, ss>>>(a, scan, part));
     MG_LAUNCH(KID_OTHER, ss, k_mss_level_end<<<1, 32, 0, ss>>>(a.ctl, h, use_h));
   };
   LoopResult res;
