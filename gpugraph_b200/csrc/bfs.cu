@@ -91,6 +91,108 @@ __global__ void __launch_bounds__(kNT, 6) k_bfs_pull(GasArgs<BfsP> a) {
   if (lane == 0 && my_edges) atomicAdd(&ctl->next_edges, my_edges);
 }
 
+// Top-down level of the bfs program (the engine's expand + contract with the
+// bfs functors, Algorithms/BFS/bfs.h:233-286, fused and specialised): tiles of
+// NV = kNT*VT items (frontier vertices and their out-edges) from the frontier
+// scan's merge-path partition. Every thread takes its VT items through three
+// batches of independent memory operations instead of VT dependent chains:
+// all column loads, then all visited-word loads, then the test-and-set
+// atomics of the unvisited ones; a winner writes its depth and its bit in the
+// next frontier bitmap (which a following bottom-up level reads) and is
+// compacted into the next queue.
+template <int VT>
+__global__ void __launch_bounds__(kNT, 6) k_bfs_push(GasArgs<BfsP> a) {
+  constexpr int NV = kNT * VT;
+  __shared__ int32_t s_v[NV + 1];
+  __shared__ int32_t s_base[NV + 1];
+  __shared__ int32_t s_rs[NV + 1];
+  __shared__ int32_t s_own[NV];
+  __shared__ uint32_t s_cnt[VT * kNW + 1];
+  __shared__ uint32_t s_tile, s_prefix, s_warpmax[kNW];
+  __shared__ int s_fail;
+  __shared__ unsigned long long s_edges;
+  Ctl *ctl = a.ctl;
+  if (!ctl->active || ctl->mode != MODE_QUEUE) return;
+  const uint32_t level = ctl->level, n = ctl->frontier_size, total = ctl->edge_total;
+  const uint32_t ntiles = ctl->exp_tiles, epoch = ctl->epoch + 1;
+  const unsigned long long spin_limit = ctl->spin_limit;
+  const bool ordered = ctl->ordered != 0;
+  const unsigned long long items = (unsigned long long)n + total;
+  const int32_t *F = cur_queue(a, level);
+  int32_t *Fout = nxt_queue(a, level);
+  uint32_t *next_bm = nxt_bm(a, level);
+  uint32_t *visited = a.vl.d_visited;
+  int32_t *labels = a.vl.d_labels;
+  const int32_t *ro = a.g.row_offsets, *col = a.g.col;
+  const int32_t V = a.g.V;
+  const int lane = lane_id();
+  unsigned long long my_edges = 0, my_bytes = 0;
+  if (threadIdx.x == 0) {
+    s_fail = 0;
+    s_edges = 0;
+  }
+  for (;;) {
+    const uint32_t tile = next_tile(&ctl->tile_ctr[1], &s_tile);
+    if (tile >= ntiles || s_fail) break;
+    int cnt;
+    if (!decode_tile<VT>(tile, ntiles, n, items, a.part, a.scan, F, ro, s_v, s_base, s_rs, s_own, s_warpmax, &cnt,
+                         [](int, int) {})) {
+      if (threadIdx.x == 0) {
+        raise_error(ctl, MG_ERR_OVERFLOW);
+        s_fail = 1;
+      }
+      __syncthreads();
+      break;
+    }
+    int32_t nbr[VT];
+#pragma unroll
+    for (int r = 0; r < VT; ++r) {
+      const int k = r * kNT + threadIdx.x;
+      nbr[r] = -1;
+      if (k < cnt) {
+        const int j = s_own[k];
+        const int el = k - s_base[j] - 1;
+        my_bytes += el >= 0 ? 8ull : 12ull;  // column + visited probe; a vertex's own item: its offsets + queue entry
+        if (el >= 0) {
+          const int eid = s_rs[j] + el;
+          if ((unsigned)eid < (unsigned)a.g.E) nbr[r] = col[eid];
+          else raise_error(ctl, MG_ERR_OVERFLOW);
+        }
+      }
+    }
+    uint32_t word[VT];
+#pragma unroll
+    for (int r = 0; r < VT; ++r) word[r] = ((unsigned)nbr[r] < (unsigned)V) ? ld_volatile(&visited[nbr[r] >> 5]) : ~0u;
+    uint32_t bal[VT];
+    int32_t outv[VT];
+#pragma unroll
+    for (int r = 0; r < VT; ++r) {
+      bool surv = false;
+      const int u = nbr[r];
+      if ((unsigned)u < (unsigned)V) {
+        const uint32_t bit = 1u << (u & 31);
+        if (!(word[r] & bit)) surv = !(atomicOr(&visited[u >> 5], bit) & bit);
+      }
+      if (surv) {
+        labels[u] = (int)level + 1;
+        atomicOr(&next_bm[u >> 5], 1u << (u & 31));
+        my_edges += (unsigned long long)(ro[u + 1] - ro[u]);
+        my_bytes += 8;  // queue entry + depth
+      }
+      bal[r] = __ballot_sync(0xffffffffu, surv);
+      outv[r] = u;
+    }
+    if (!tile_enqueue<VT>(bal, outv, s_cnt, &s_prefix, &s_fail, ordered, a.status, tile, ntiles, epoch, spin_limit,
+                          Fout, (uint32_t)V, ctl))
+      break;
+  }
+  add_bytes(ctl->kbytes, KID_EXPAND, my_bytes);
+  my_edges = warp_sum(my_edges);
+  if (lane == 0 && my_edges) atomicAdd(&s_edges, my_edges);
+  __syncthreads();
+  if (threadIdx.x == 0 && s_edges) atomicAdd(&ctl->next_edges, s_edges);
+}
+
 // Predecessors after a BFS, the rule of the reference's pred_extract
 // (Algorithms/BFS/predextract.cuh:143-154 gather_edge, :211-218 max reduce,
 // :236 empty in-lists): pred[v] = max(-1, max over in-neighbours u with
@@ -317,6 +419,8 @@ int bfs_run(mg_graph *g, const std::vector<int32_t> &roots, int32_t *depths, mg_
   const int grid = persistent_grid(g, o, 4);
   // the pull kernel holds no shared memory and at most 40 registers: 48 warps per SM
   const int pull_grid = g->num_sms * 6;
+  // the push kernel: at most 40 registers and 25 KB of shared memory, 6 CTAs per SM
+  const int push_grid = std::max(grid, g->num_sms * 6);
   k_fill_i32<<<g->num_sms * 4, 256, 0, s>>>(w.vbuf[0], BfsP::INIT_VALUE, V);
   k_ctl_init<<<1, 32, 0, s>>>(w.ctl, nsrc, max_iter, (unsigned long long)o->spin_limit, MODE_QUEUE, ctl_flags(o));
   k_bfs_init<<<1, 256, 0, s>>>(w.ctl, w.queue[0], (int32_t)nsrc, w.vbuf[0], w.visited, w.bm[0], g->csr.row_offsets,
@@ -331,10 +435,10 @@ int bfs_run(mg_graph *g, const std::vector<int32_t> &roots, int32_t *depths, mg_
     MG_LAUNCH(KID_CONVERT, ss, k_bm_to_queue<<<grid, kNT, 0, ss>>>(a));
     if (small_tiles) {
       MG_LAUNCH(KID_SCAN, ss, (k_frontier_scan<BfsP, kVTS, 4><<<grid, kNT, 0, ss>>>(a)));
-      MG_LAUNCH(KID_EXPAND, ss, (k_expand<BfsP, 4><<<grid, kNT, 0, ss>>>(a)));
+      MG_LAUNCH(KID_EXPAND, ss, (k_bfs_push<4><<<push_grid, kNT, 0, ss>>>(a)));
     } else {
       MG_LAUNCH(KID_SCAN, ss, (k_frontier_scan<BfsP, kVTS, kVT><<<grid, kNT, 0, ss>>>(a)));
-      MG_LAUNCH(KID_EXPAND, ss, (k_expand<BfsP, kVT><<<grid, kNT, 0, ss>>>(a)));
+      MG_LAUNCH(KID_EXPAND, ss, (k_bfs_push<kVT><<<push_grid, kNT, 0, ss>>>(a)));
     }
     MG_LAUNCH(KID_BFS_PULL, ss, k_bfs_pull<<<pull_grid, kNT, 0, ss>>>(a));
     MG_LAUNCH(KID_OTHER, ss, k_bfs_level_end<<<1, 32, 0, ss>>>(a.ctl, Vv, E, h, use_h));

@@ -308,6 +308,73 @@ MG_DEVINL bool decode_tile(uint32_t tile, uint32_t ntiles, uint32_t n, unsigned 
   return true;
 }
 
+// ------------------------------------------------------ tile compaction ---
+// Appends a tile's surviving items to the next queue. bal[r]/outv[r]: each
+// warp's round-r survivor ballot and item. The (round, warp) counts are
+// scanned by warp 0, then either one atomic reservation per tile places the
+// tile (no tile waits for another) or, with `ordered`, a decoupled look-back
+// over tiles keeps the queue in tile order. Called by all kNT threads; returns
+// false when the look-back gave up (the error is raised).
+template <int VT>
+MG_DEVINL bool tile_enqueue(const uint32_t (&bal)[VT], const int32_t (&outv)[VT], uint32_t *s_cnt,
+                            uint32_t *s_prefix, int *s_fail, bool ordered, unsigned long long *status, uint32_t tile,
+                            uint32_t ntiles, uint32_t epoch, unsigned long long spin_limit, int32_t *Fout, uint32_t V,
+                            Ctl *ctl) {
+  const int lane = lane_id(), warp = warp_id();
+  if (lane == 0) {
+#pragma unroll
+    for (int r = 0; r < VT; ++r) s_cnt[r * kNW + warp] = __popc(bal[r]);
+  }
+  __syncthreads();
+  if (warp == 0) {
+    // Exclusive scan over the VT*kNW (round, warp) counts; 2 per lane for VT*kNW <= 64.
+    constexpr int C = VT * kNW;
+    constexpr int PER = (C + 31) / 32;
+    uint32_t x[PER];
+    uint32_t s = 0;
+#pragma unroll
+    for (int q = 0; q < PER; ++q) {
+      const int idx = lane * PER + q;
+      x[q] = idx < C ? s_cnt[idx] : 0u;
+      s += x[q];
+    }
+    const uint32_t inc = warp_inclusive_sum(s);
+    uint32_t run = inc - s;
+#pragma unroll
+    for (int q = 0; q < PER; ++q) {
+      const int idx = lane * PER + q;
+      if (idx < C) s_cnt[idx] = run;
+      run += x[q];
+    }
+    const uint32_t tile_total = __shfl_sync(0xffffffffu, inc, 31);
+    if (ordered) {
+      bool failed = false;
+      const uint32_t pre = lookback(status, tile, tile_total, epoch, spin_limit, &failed);
+      if (lane == 0) {
+        *s_prefix = pre;
+        if (failed) {
+          *s_fail = 1;
+          raise_error(ctl, MG_ERR_TIMEOUT);
+        } else if (tile == ntiles - 1) {
+          ctl->next_size = pre + tile_total;
+        }
+      }
+    } else if (lane == 0) {
+      *s_prefix = tile_total ? atomicAdd(&ctl->next_size, tile_total) : 0u;
+    }
+  }
+  __syncthreads();
+  if (*s_fail) return false;
+#pragma unroll
+  for (int r = 0; r < VT; ++r) {
+    if ((bal[r] >> lane) & 1u) {
+      const uint32_t pos = *s_prefix + s_cnt[r * kNW + warp] + __popc(bal[r] & lanemask_lt());
+      if (pos < V) Fout[pos] = outv[r];
+    }
+  }
+  return true;
+}
+
 // ------------------------------------------------------ expand + contract ---
 template <class P, int VT>
 __global__ void __launch_bounds__(kNT) k_expand(GasArgs<P> a) {
@@ -401,57 +468,10 @@ __global__ void __launch_bounds__(kNT) k_expand(GasArgs<P> a) {
       bal[r] = __ballot_sync(0xffffffffu, surv);
       outv[r] = fo;
       if (surv) my_bytes += 8;  // queue entry + the Program's per-vertex write
-      if (lane == 0) s_cnt[r * kNW + warp] = __popc(bal[r]);
     }
-    __syncthreads();
-    if (warp == 0) {
-      // Exclusive scan over the VT*kNW (round, warp) counts; 2 per lane for VT*kNW <= 64.
-      constexpr int C = VT * kNW;
-      constexpr int PER = (C + 31) / 32;
-      uint32_t x[PER];
-      uint32_t s = 0;
-#pragma unroll
-      for (int q = 0; q < PER; ++q) {
-        const int idx = lane * PER + q;
-        x[q] = idx < C ? s_cnt[idx] : 0u;
-        s += x[q];
-      }
-      const uint32_t inc = warp_inclusive_sum(s);
-      uint32_t run = inc - s;
-#pragma unroll
-      for (int q = 0; q < PER; ++q) {
-        const int idx = lane * PER + q;
-        if (idx < C) s_cnt[idx] = run;
-        run += x[q];
-      }
-      const uint32_t tile_total = __shfl_sync(0xffffffffu, inc, 31);
-      if (ordered) {
-        // Deterministic frontier order: decoupled look-back over tiles.
-        bool failed = false;
-        const uint32_t pre = lookback(a.status, tile, tile_total, epoch, spin_limit, &failed);
-        if (lane == 0) {
-          s_prefix = pre;
-          if (failed) {
-            s_fail = 1;
-            raise_error(ctl, MG_ERR_TIMEOUT);
-          } else if (tile == ntiles - 1) {
-            ctl->next_size = pre + tile_total;
-          }
-        }
-      } else if (lane == 0) {
-        // One atomic reservation per tile: no tile waits for another.
-        s_prefix = tile_total ? atomicAdd(&ctl->next_size, tile_total) : 0u;
-      }
-    }
-    __syncthreads();
-    if (s_fail) break;
-#pragma unroll
-    for (int r = 0; r < VT; ++r) {
-      if ((bal[r] >> lane) & 1u) {
-        const uint32_t pos = s_prefix + s_cnt[r * kNW + warp] + __popc(bal[r] & lanemask_lt());
-        if (pos < (uint32_t)V) Fout[pos] = outv[r];
-      }
-    }
+    if (!tile_enqueue<VT>(bal, outv, s_cnt, &s_prefix, &s_fail, ordered, a.status, tile, ntiles, epoch, spin_limit,
+                          Fout, (uint32_t)V, ctl))
+      break;
   }
   add_bytes(ctl->kbytes, KID_EXPAND, my_bytes);
   if (track_next_edges_trait<P>::value) {
