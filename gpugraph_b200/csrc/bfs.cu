@@ -108,7 +108,7 @@ __global__ void __launch_bounds__(kNT, 6) k_bfs_push(GasArgs<BfsP> a) {
   __shared__ int32_t s_rs[NV + 1];
   __shared__ int32_t s_own[NV];
   __shared__ uint32_t s_cnt[VT * kNW + 1];
-  __shared__ uint32_t s_tile, s_prefix, s_warpmax[kNW];
+  __shared__ uint32_t s_tile, s_prefix;
   __shared__ int s_fail;
   __shared__ unsigned long long s_edges;
   Ctl *ctl = a.ctl;
@@ -135,7 +135,7 @@ __global__ void __launch_bounds__(kNT, 6) k_bfs_push(GasArgs<BfsP> a) {
     const uint32_t tile = next_tile(&ctl->tile_ctr[1], &s_tile);
     if (tile >= ntiles || s_fail) break;
     int cnt;
-    if (!decode_tile<VT>(tile, ntiles, n, items, a.part, a.scan, F, ro, s_v, s_base, s_rs, s_own, s_warpmax, &cnt,
+    if (!decode_tile<VT>(tile, ntiles, n, items, a.part, a.scan, F, ro, s_v, s_base, s_rs, s_own, &cnt,
                          [](int, int) {})) {
       if (threadIdx.x == 0) {
         raise_error(ctl, MG_ERR_OVERFLOW);

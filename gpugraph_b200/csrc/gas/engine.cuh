@@ -247,18 +247,17 @@ __global__ void __launch_bounds__(kNT) k_frontier_scan(GasArgs<P> a) {
 }
 
 // ------------------------------------------------------------ tile decode --
-// Loads the frontier blocks of expand tile `tile` into shared memory and marks
-// the owner block of every item (inclusive max-scan of block start markers),
-// so item k of the tile is edge (k - s_base[s_own[k]] - 1) of vertex
+// Loads the frontier blocks of expand tile `tile` into shared memory and finds
+// the owner block of every item (the last block starting at or before it), so
+// item k of the tile is edge (k - s_base[s_own[k]] - 1) of vertex
 // s_v[s_own[k]] (negative: the vertex's own item). per_block(j, v) runs once per
 // loaded block. Returns false (nothing decoded) on an inconsistent partition.
 // Must be called by all kNT threads; ends with __syncthreads().
 template <int VT, class PerBlock>
 MG_DEVINL bool decode_tile(uint32_t tile, uint32_t ntiles, uint32_t n, unsigned long long items, const int32_t *part,
                            const uint32_t *scan, const int32_t *F, const int32_t *ro, int32_t *s_v, int32_t *s_base,
-                           int32_t *s_rs, int32_t *s_own, uint32_t *s_warpmax, int *cnt_out, PerBlock per_block) {
+                           int32_t *s_rs, int32_t *s_own, int *cnt_out, PerBlock per_block) {
   constexpr int NV = kNT * VT;
-  const int lane = lane_id(), warp = warp_id();
   const unsigned long long d0 = (unsigned long long)tile * NV;
   const int cnt = (int)((items - d0) < (unsigned long long)NV ? (items - d0) : (unsigned long long)NV);
   const int i0 = part[tile];
@@ -275,35 +274,28 @@ MG_DEVINL bool decode_tile(uint32_t tile, uint32_t ntiles, uint32_t n, unsigned 
     s_rs[j] = ro[v];
     per_block(j, v);
   }
-  for (int k = threadIdx.x; k < NV; k += kNT) s_own[k] = 0;
   __syncthreads();
-  for (int j = 1 + threadIdx.x; j < nblk; j += kNT) {
-    const int b = s_base[j];
-    if (b >= 0 && b < cnt) s_own[b] = j;
-  }
-  __syncthreads();
-  int loc[VT];
-  int m = 0;
+  // Owners: thread t covers items [t*VT, t*VT+VT). Block starts (s_base) are
+  // increasing and block 0 starts at or before the tile, so the owner of the
+  // first item is the last block starting at or before it (binary search); the
+  // next VT-1 items walk forward.
+  const int k0 = threadIdx.x * VT;
+  if (k0 < cnt) {
+    int lo = 0, hi = nblk - 1;
+    while (lo < hi) {
+      const int mid = (lo + hi + 1) >> 1;
+      if (s_base[mid] <= k0) lo = mid;
+      else hi = mid - 1;
+    }
 #pragma unroll
-  for (int r = 0; r < VT; ++r) {
-    int x = s_own[threadIdx.x * VT + r];
-    m = x > m ? x : m;
-    loc[r] = m;
+    for (int r = 0; r < VT; ++r) {
+      const int k = k0 + r;
+      if (k < cnt) {
+        while (lo + 1 < nblk && s_base[lo + 1] <= k) ++lo;
+        s_own[k] = lo;
+      }
+    }
   }
-  int wm = m;
-#pragma unroll
-  for (int o = 1; o < 32; o <<= 1) {
-    int y = __shfl_up_sync(0xffffffffu, wm, o);
-    if (lane >= o) wm = y > wm ? y : wm;
-  }
-  if (lane == 31) s_warpmax[warp] = (uint32_t)wm;
-  __syncthreads();
-  int carry = 0;
-  for (int w = 0; w < warp; ++w) carry = (int)s_warpmax[w] > carry ? (int)s_warpmax[w] : carry;
-  int prev = __shfl_up_sync(0xffffffffu, wm, 1);
-  if (lane > 0) carry = prev > carry ? prev : carry;
-#pragma unroll
-  for (int r = 0; r < VT; ++r) s_own[threadIdx.x * VT + r] = loc[r] > carry ? loc[r] : carry;
   __syncthreads();
   return true;
 }
@@ -385,7 +377,7 @@ __global__ void __launch_bounds__(kNT) k_expand(GasArgs<P> a) {
   __shared__ int32_t s_own[NV];
   __shared__ uint8_t s_ch[NV + 1];
   __shared__ uint32_t s_cnt[VT * kNW + 1];
-  __shared__ uint32_t s_tile, s_prefix, s_warpmax[kNW];
+  __shared__ uint32_t s_tile, s_prefix;
   __shared__ int s_fail;
   __shared__ unsigned long long s_edges;
   Ctl *ctl = a.ctl;
@@ -414,7 +406,7 @@ __global__ void __launch_bounds__(kNT) k_expand(GasArgs<P> a) {
     const uint32_t tile = next_tile(&ctl->tile_ctr[1], &s_tile);
     if (tile >= ntiles || s_fail) break;
     int cnt;
-    if (!decode_tile<VT>(tile, ntiles, n, items, a.part, a.scan, F, ro, s_v, s_base, s_rs, s_own, s_warpmax, &cnt,
+    if (!decode_tile<VT>(tile, ntiles, n, items, a.part, a.scan, F, ro, s_v, s_base, s_rs, s_own, &cnt,
                          [&](int j, int v) { s_ch[j] = (uint8_t)ev(v, (char)a.changed[v], a.vl, a.el); })) {
       // Inconsistent partition (cannot happen for a well-formed scan): record
       // it and stop instead of indexing out of bounds.

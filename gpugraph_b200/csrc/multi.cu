@@ -539,7 +539,7 @@ __global__ void __launch_bounds__(kNT) k_mss_expand(MultiArgs a, const uint32_t 
   __shared__ int32_t s_base[NV + 1];
   __shared__ int32_t s_rs[NV + 1];
   __shared__ int32_t s_own[NV];
-  __shared__ uint32_t s_tile, s_warpmax[kNW];
+  __shared__ uint32_t s_tile;
   __shared__ int s_fail;
   Ctl *ctl = a.ctl;
   if (!ctl->active) return;
@@ -559,7 +559,7 @@ __global__ void __launch_bounds__(kNT) k_mss_expand(MultiArgs a, const uint32_t 
     const uint32_t tile = next_tile(&ctl->tile_ctr[1], &s_tile);
     if (tile >= ntiles || s_fail) break;
     int cnt;
-    if (!decode_tile<VT>(tile, ntiles, n, items, part, scan, Q, ro, s_v, s_base, s_rs, s_own, s_warpmax, &cnt,
+    if (!decode_tile<VT>(tile, ntiles, n, items, part, scan, Q, ro, s_v, s_base, s_rs, s_own, &cnt,
                          [](int, int) {})) {
       if (threadIdx.x == 0) {
         raise_error(ctl, MG_ERR_OVERFLOW);
