@@ -35,7 +35,8 @@ class Options(C.Structure):
         ("pad0", C.c_int32),
         ("alpha_multi", C.c_double),
         ("ordered_frontier", C.c_int32),
-        ("reserved", C.c_int32 * 3),
+        ("generic_engine", C.c_int32),
+        ("reserved", C.c_int32 * 2),
     ]
 
 

@@ -18,6 +18,7 @@
 namespace mg {
 
 int cc_union_find(mg_graph *g, int32_t *labels, mg_stats *stats, const mg_options *o);  // cc.cu
+int sssp_fused(mg_graph *g, int32_t src, int32_t *dists, mg_stats *stats, const mg_options *o);  // sssp.cu
 
 __global__ void k_fill_u32(uint32_t *p, uint32_t v, int64_t n) {
   for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
@@ -56,6 +57,8 @@ int mg_sssp(mg_graph *g, int32_t src, int32_t *dists, mg_stats *stats, const mg_
   std::vector<int32_t> roots;
   int st = check_sources(g, &src, 1, &roots);
   if (st != MG_OK) return st;
+  if (!dists) return set_error(MG_ERR_ARG, "dists is NULL");
+  if (!o->generic_engine) return sssp_fused(g, src, dists, stats, o);  // sssp.cu
   cudaStream_t s = run_stream(g, o);
   if ((st = prepare_run(g, s)) != MG_OK) return st;
   using P = programs::sssp;
@@ -94,7 +97,7 @@ int mg_cc(mg_graph *g, int32_t *labels, mg_stats *stats, const mg_options *opts)
   mg_options d;
   const mg_options *o = opts_or_default(opts, &d);
   // symmetric graph: the same labels in one union-find pass (cc.cu)
-  if (!g->directed) return cc_union_find(g, labels, stats, o);
+  if (!g->directed && !o->generic_engine) return cc_union_find(g, labels, stats, o);
   cudaStream_t s = run_stream(g, o);
   int st = prepare_run(g, s);
   if (st != MG_OK) return st;

@@ -72,7 +72,9 @@ typedef struct mg_options {
                                 edges exceed edges / alpha_multi */
   int32_t ordered_frontier;  /* 1: next frontiers keep a deterministic order (decoupled
                                 look-back); 0: one atomic reservation per tile */
-  int32_t reserved[3];
+  int32_t generic_engine;    /* 1: mg_sssp / mg_cc run the bundled GAS Program through the
+                                generic engine; 0: the specialised kernels (same results) */
+  int32_t reserved[2];
 } mg_options;
 
 /* Per-run statistics (reference: Statistics::stats_per_iter, GASengine/statistics.h:31-81). */

@@ -200,3 +200,21 @@ def test_bfs_pred_matches_oracle(kind):
                    "mg_bfs_pred")
         assert np.array_equal(pd.cpu().numpy(), p) and np.array_equal(dd.cpu().numpy(), d)
     g.close()
+
+
+@pytest.mark.parametrize("generic", [0, 1])
+def test_specialised_and_generic_engine_agree(generic):
+    # mg_sssp / mg_cc run fused kernels by default and the bundled GAS Programs through the
+    # generic engine with generic_engine=1: both give the oracle's results.
+    hg = HostGraph.rmat(14, 8, seed=12).with_weights(1, 64, seed=12)
+    g = Graph(hg)
+    for s in (hg.max_degree_vertex(), 5):
+        d, st = g.sssp(s, generic_engine=generic)
+        assert np.array_equal(d, oracle.sssp(hg.row_offsets, hg.column_indices, hg.edge_values, s))
+        assert st["converged"] == 1
+    labels, _ = g.cc(generic_engine=generic)
+    assert np.array_equal(labels, oracle.cc(hg.row_offsets, hg.column_indices))
+    road = HostGraph.road_grid(90, 0.02, 0.005, seed=13).with_weights(1, 1000, seed=13)
+    gr = Graph(road)
+    d, _ = gr.sssp(77, generic_engine=generic)
+    assert np.array_equal(d, oracle.sssp(road.row_offsets, road.column_indices, road.edge_values, 77))
