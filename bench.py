@@ -464,8 +464,8 @@ def cpu_bfs_sample(hg, srcs, cores: int):
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=5)
-    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--steps", type=int, default=100)
+    ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="native", choices=["native", "reference"])
     ap.add_argument("--scale", type=int, default=SCALE)
     ap.add_argument("--quick", action="store_true", help="skip the SSSP/CC sub-results")
