@@ -203,6 +203,14 @@ constexpr int kMsSub = 4;     // 32-edge sub-chunks whose loads are in flight to
 MG_DEVINL void ms_segment(u64 x, int ck, int b, int e, bool starts, bool take, uint32_t le, u64 &acc) {
   const int p = b - ck;
   const uint32_t head = __reduce_or_sync(0xffffffffu, (starts && p >= 0 && p < 32) ? 1u << p : 0u) | 1u;
+  if (head == 1u) {
+    // no list starts inside the sub-chunk: one list holds all of it (positions
+    // past the pulling lists carry 0), so a plain warp OR is its part
+    const u64 all = ((u64)__reduce_or_sync(0xffffffffu, (uint32_t)(x >> 32)) << 32) |
+                    __reduce_or_sync(0xffffffffu, (uint32_t)x);
+    if (take && max(b, ck) < min(e, ck + 32)) acc |= all;
+    return;
+  }
 #pragma unroll
   for (int d = 1; d < 32; d <<= 1) {
     const u64 t = __shfl_up_sync(0xffffffffu, x, d);
