@@ -23,7 +23,14 @@ using BfsP = programs::bfs;
 constexpr int kVTS = 4;  // frontier entries per thread in the scan
 constexpr int kVT = 8;   // items per thread in the expand (NV = 2048)
 
-// Bottom-up level: warp per 32-vertex bitmap word, lane per vertex.
+// Bottom-up level: a warp takes kPullWords consecutive 32-vertex bitmap words
+// per ticket (lane = vertex within a word). For every unvisited vertex the
+// first four in-edges of all the warp's words are probed at once (their row
+// indices, then their frontier-bitmap words), so one round trip serves
+// kPullWords x 32 vertices; the in-lists are ordered hubs first, so most
+// vertices with a parent find it there. Vertices still searching continue four
+// in-edges per step and stop at the first parent.
+constexpr int kPullWords = 4;
 __global__ void __launch_bounds__(kNT, 6) k_bfs_pull(GasArgs<BfsP> a) {
   Ctl *ctl = a.ctl;
   if (!ctl->active || ctl->mode != MODE_BITMAP) return;
@@ -33,55 +40,87 @@ __global__ void __launch_bounds__(kNT, 6) k_bfs_pull(GasArgs<BfsP> a) {
   uint32_t *visited = a.vl.d_visited;
   const int32_t V = a.g.V;
   const uint32_t words = ((uint32_t)V + 31) / 32;
+  const uint32_t tickets = (words + kPullWords - 1) / kPullWords;
   const int32_t *coff = a.g.csc_offsets, *crow = a.g.pull_rows, *ro = a.g.row_offsets;
   const int lane = lane_id();
   unsigned long long my_cnt = 0, my_edges = 0, my_bytes = 0;
-  // 32-vertex words are handed out dynamically (one atomic per word); the
-  // ticket for the next word is drawn while the current one is processed
+  // tickets (kPullWords words each) are handed out dynamically; the next one
+  // is drawn while the current one is processed
   uint32_t ticket = 0;
   if (lane == 0) ticket = atomicAdd(&ctl->group_ctr, 1u);
   for (;;) {
-    const uint32_t w = __shfl_sync(0xffffffffu, ticket, 0);
-    if (w >= words) break;
+    const uint32_t t = __shfl_sync(0xffffffffu, ticket, 0);
+    if (t >= tickets) break;
     if (lane == 0) ticket = atomicAdd(&ctl->group_ctr, 1u);
-    const uint32_t vis = visited[w];
-    const int v = (int)(w * 32 + lane);
-    bool found = false;
-    if (v < V && !((vis >> lane) & 1u)) {
-      const int beg = coff[v], end = coff[v + 1];
-      int e = beg;
-      // four in-edges per step (independent loads in flight); stop at the
-      // first step that finds a parent
-      while (e < end) {
-        const int c = min(4, end - e);
-        const int u0 = crow[e];
-        const int u1 = c > 1 ? crow[e + 1] : u0;
-        const int u2 = c > 2 ? crow[e + 2] : u0;
-        const int u3 = c > 3 ? crow[e + 3] : u0;
-        const uint32_t hit = ((__ldg(&cur[u0 >> 5]) >> (u0 & 31)) | (__ldg(&cur[u1 >> 5]) >> (u1 & 31)) |
-                              (__ldg(&cur[u2 >> 5]) >> (u2 & 31)) | (__ldg(&cur[u3 >> 5]) >> (u3 & 31))) &
-                             1u;
-        e += c;
-        if (hit) {
-          found = true;
-          e -= 1;  // byte count below adds the found edge back
-          break;
+    uint32_t vis[kPullWords];
+    int beg[kPullWords], end[kPullWords];
+#pragma unroll
+    for (int q = 0; q < kPullWords; ++q) {
+      const uint32_t w = t * kPullWords + q;
+      const int v = (int)(w * 32 + lane);
+      vis[q] = w < words ? visited[w] : ~0u;
+      beg[q] = v < V ? coff[v] : 0;
+      end[q] = v < V ? coff[v + 1] : 0;
+    }
+    // first step for every word at once: up to four in-edges per searching vertex
+    int u[kPullWords][4];
+    bool search[kPullWords];
+#pragma unroll
+    for (int q = 0; q < kPullWords; ++q) {
+      const int v = (int)((t * kPullWords + q) * 32 + lane);
+      search[q] = v < V && !((vis[q] >> lane) & 1u);
+      if (!search[q]) end[q] = beg[q];  // nothing to scan
+#pragma unroll
+      for (int k = 0; k < 4; ++k) u[q][k] = beg[q] + k < end[q] ? crow[beg[q] + k] : -1;
+    }
+    bool found[kPullWords];
+#pragma unroll
+    for (int q = 0; q < kPullWords; ++q) {
+      uint32_t hit = 0;
+#pragma unroll
+      for (int k = 0; k < 4; ++k)
+        if (u[q][k] >= 0) hit |= __ldg(&cur[u[q][k] >> 5]) >> (u[q][k] & 31);
+      found[q] = hit & 1u;
+    }
+#pragma unroll
+    for (int q = 0; q < kPullWords; ++q) {
+      const uint32_t w = t * kPullWords + q;
+      const int v = (int)(w * 32 + lane);
+      int e = min(beg[q] + 4, end[q]);
+      int probed = e - beg[q];
+      if (!found[q]) {
+        // continue four in-edges per step (independent loads in flight)
+        while (e < end[q]) {
+          const int c = min(4, end[q] - e);
+          const int u0 = crow[e];
+          const int u1 = c > 1 ? crow[e + 1] : u0;
+          const int u2 = c > 2 ? crow[e + 2] : u0;
+          const int u3 = c > 3 ? crow[e + 3] : u0;
+          const uint32_t hit = ((__ldg(&cur[u0 >> 5]) >> (u0 & 31)) | (__ldg(&cur[u1 >> 5]) >> (u1 & 31)) |
+                                (__ldg(&cur[u2 >> 5]) >> (u2 & 31)) | (__ldg(&cur[u3 >> 5]) >> (u3 & 31))) &
+                               1u;
+          e += c;
+          probed += c;
+          if (hit) {
+            found[q] = true;
+            break;
+          }
         }
       }
       // offsets + per inspected edge: row index and frontier-bitmap word
-      my_bytes += 8 + 8ull * (unsigned long long)(e - beg + (found ? 1 : 0));
-    }
-    const uint32_t bal = __ballot_sync(0xffffffffu, found);
-    if (lane == 0) {
-      nxt[w] = bal;
-      if (bal) visited[w] = vis | bal;
-      my_cnt += __popc(bal);
-    }
-    if (lane == 0) my_bytes += 8;  // visited word + next-frontier word
-    if (found) {
-      my_bytes += 4;
-      a.vl.d_labels[v] = (int)level + 1;
-      my_edges += (unsigned long long)(ro[v + 1] - ro[v]);
+      if (search[q]) my_bytes += 8 + 8ull * (unsigned long long)probed;
+      const uint32_t bal = __ballot_sync(0xffffffffu, found[q]);
+      if (lane == 0 && w < words) {
+        nxt[w] = bal;
+        if (bal) visited[w] = vis[q] | bal;
+        my_cnt += __popc(bal);
+        my_bytes += 8;  // visited word + next-frontier word
+      }
+      if (found[q]) {
+        my_bytes += 4;
+        a.vl.d_labels[v] = (int)level + 1;
+        my_edges += (unsigned long long)(ro[v + 1] - ro[v]);
+      }
     }
   }
   add_bytes(ctl->kbytes, KID_BFS_PULL, my_bytes);
