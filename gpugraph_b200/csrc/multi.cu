@@ -198,8 +198,8 @@ constexpr int kMsSub = 4;     // 32-edge sub-chunks whose loads are in flight to
 // OR scan with a head at every non-empty list start in the sub-chunk (and at
 // lane 0) leaves the OR of each list's part at its last lane, which the list's
 // owner takes when it is still pulling. A step of offset d ORs lane i-d into
-// lane i when no head lies in (i-d, i]: with le = lanes [0, i] that window is
-// le & ~(le >> d), and for i < d it takes in lane 0, which is always a head.
+// lane i when no head lies in (i-d, i], i.e. when i minus the last head at or
+// before i (le = lanes [0, i]) is at least d.
 MG_DEVINL void ms_segment(u64 x, int ck, int b, int e, bool starts, bool take, uint32_t le, u64 &acc) {
   const int p = b - ck;
   const uint32_t head = __reduce_or_sync(0xffffffffu, (starts && p >= 0 && p < 32) ? 1u << p : 0u) | 1u;
@@ -211,10 +211,13 @@ MG_DEVINL void ms_segment(u64 x, int ck, int b, int e, bool starts, bool take, u
     if (take && max(b, ck) < min(e, ck + 32)) acc |= all;
     return;
   }
+  // distance from this lane back to the head of its segment: a step of offset
+  // d ORs lane i-d in while that lane is still in the segment
+  const int run = (31 - __clz(le)) - (31 - __clz(head & le));
 #pragma unroll
   for (int d = 1; d < 32; d <<= 1) {
     const u64 t = __shfl_up_sync(0xffffffffu, x, d);
-    if ((head & le & ~(le >> d)) == 0u) x |= t;
+    if (run >= d) x |= t;
   }
   const int q = min(e, ck + 32) - 1 - ck;
   const u64 t = __shfl_sync(0xffffffffu, x, q < 0 ? 0 : (q > 31 ? 31 : q));
