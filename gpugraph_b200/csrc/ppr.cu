@@ -7,14 +7,17 @@
 // Adjoint:  for L with G = dL/dR, lambda = G + d P lambda, pulled over the
 //           out-edges (CSR): lambda'[u,:] = G[u,:] + d * sum_{u->v} w(u,v) lambda[v,:]
 //           dL/dT = (1-d) lambda,  dL/dw(u,v) = d * <lambda[v,:], R[u,:]>
-// Both solves stop when the L1 change over all entries is <= tolerance * nvec,
-// or after iter_num iterations.
+// Both solves stop when the L1 change over all entries is <= tolerance times
+// the L1 norm of their right-hand side (T or G; for teleport columns that are
+// distributions that is tolerance * nvec), or after iter_num iterations.
 //
 // Layout and work split: a warp owns one chunk of one vertex's adjacency and
 // lane c owns columns c and c+32, so every edge costs one coalesced read of a
-// 128-byte row (nvec = 32) plus a broadcast index/weight load; four edges are
-// in flight per step. In-lists longer than kPprChunk are cut into chunks whose
-// partial rows are added in chunk order by a fix-up pass (deterministic).
+// 128-byte row (nvec = 32) plus a broadcast index/weight load; eight edges
+// (four for nvec > 32) are in flight per step. The forward solve reads the
+// weights gathered into CSC order once per solve. In-lists longer than
+// kPprChunk are cut into chunks whose partial rows are added in chunk order by
+// a fix-up pass (deterministic).
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -74,36 +77,30 @@ __global__ void __launch_bounds__(kNT) k_ppr_iter(PprArgs a) {
     float acc[NC];
 #pragma unroll
     for (int q = 0; q < NC; ++q) acc[q] = 0.f;
-    int k = b;
-    for (; k + 4 <= e; k += 4) {
-      int u[4];
-      float wt[4];
+    // EPS edges per step, all their loads in flight (predicated at the end of
+    // the chunk): index and weight, then the EPS gathered rows
+    constexpr int EPS = NC == 1 ? 8 : 4;
+    for (int k = b; k < e; k += EPS) {
+      int u[EPS];
+      float wt[EPS];
 #pragma unroll
-      for (int j = 0; j < 4; ++j) {
-        u[j] = a.idx[k + j];
-        wt[j] = a.w[a.eid ? a.eid[k + j] : k + j];
+      for (int j = 0; j < EPS; ++j) {
+        const bool in = k + j < e;
+        u[j] = in ? a.idx[k + j] : -1;
+        wt[j] = in ? a.w[a.eid ? a.eid[k + j] : k + j] : 0.f;
       }
-      float row[4][NC];
+      float row[EPS][NC];
 #pragma unroll
-      for (int j = 0; j < 4; ++j)
+      for (int j = 0; j < EPS; ++j)
 #pragma unroll
         for (int q = 0; q < NC; ++q) {
           const int col = lane + 32 * q;
-          row[j][q] = (col < a.nvec) ? __ldg(&xold[(int64_t)u[j] * a.nvec + col]) : 0.f;
+          row[j][q] = (u[j] >= 0 && col < a.nvec) ? __ldg(&xold[(int64_t)u[j] * a.nvec + col]) : 0.f;
         }
 #pragma unroll
-      for (int j = 0; j < 4; ++j)
+      for (int j = 0; j < EPS; ++j)
 #pragma unroll
         for (int q = 0; q < NC; ++q) acc[q] = fmaf(wt[j], row[j][q], acc[q]);
-    }
-    for (; k < e; ++k) {
-      const int u = a.idx[k];
-      const float wt = a.w[a.eid ? a.eid[k] : k];
-#pragma unroll
-      for (int q = 0; q < NC; ++q) {
-        const int col = lane + 32 * q;
-        if (col < a.nvec) acc[q] = fmaf(wt, __ldg(&xold[(int64_t)u * a.nvec + col]), acc[q]);
-      }
     }
     if (lane == 0) my_bytes += (unsigned long long)(e - b) * (8ull + 4ull * a.nvec);
     if (slot < 0) {
@@ -150,7 +147,8 @@ __global__ void __launch_bounds__(kNT) k_ppr_fixup(PprArgs a) {
   if (lane == 0 && res != 0.0) atomicAdd(&ctl->acc[1], res);
 }
 
-__global__ void k_ppr_level_end(Ctl *ctl, double tol_total, cudaGraphConditionalHandle h, int use_handle) {
+// ctl->acc[2] holds the L1 norm of the right-hand side (k_ppr_rhs_norm).
+__global__ void k_ppr_level_end(Ctl *ctl, double tol, cudaGraphConditionalHandle h, int use_handle) {
   if (threadIdx.x != 0) return;
   if (ctl->active) {
     const double res = ctl->acc[1];
@@ -158,7 +156,7 @@ __global__ void k_ppr_level_end(Ctl *ctl, double tol_total, cudaGraphConditional
     ctl->residual = res;
     ctl->level += 1;
     ctl->push_levels += 1;
-    ctl->active = (res > tol_total && ctl->level < ctl->max_iter && ctl->error == 0) ? 1u : 0u;
+    ctl->active = (res > tol * ctl->acc[2] && ctl->level < ctl->max_iter && ctl->error == 0) ? 1u : 0u;
   }
   if (use_handle) cudaGraphSetConditional(h, ctl->active);
 }
@@ -211,6 +209,15 @@ __global__ void __launch_bounds__(kNT) k_ppr_edge_grad(const int32_t *ro, const 
   add_bytes(kbytes, KID_PPR, my_bytes);
 }
 
+// L1 norm of the right-hand side into ctl->acc[2] (FP64 accumulation).
+__global__ void k_ppr_rhs_norm(const float *rhs, int64_t n, Ctl *ctl) {
+  double sum = 0.0;
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+    sum += fabs((double)rhs[i]);
+  sum = warp_sum(sum);
+  if (lane_id() == 0 && sum != 0.0) atomicAdd(&ctl->acc[2], sum);
+}
+
 __global__ void k_scale_copy(const float *src, float *dst, float s, int64_t n) {
   for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
     dst[i] = s * src[i];
@@ -219,6 +226,11 @@ __global__ void k_scale_copy(const float *src, float *dst, float s, int64_t n) {
 __global__ void k_copy_f32(const float *src, float *dst, int64_t n) {
   for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
     dst[i] = src[i];
+}
+
+__global__ void k_gather_f32(const int32_t *idx, const float *src, float *dst, int64_t n) {
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+    dst[i] = src[idx[i]];
 }
 
 // Chunk plan for the solve over `off` (host copy of the offsets).
@@ -314,14 +326,17 @@ static int ppr_solve(mg_graph *g, int dir, const float *w, const float *rhs, flo
   // from the graph's own buffers, so callers may pass different pointers.
   const int64_t n = (int64_t)g->nodes * nvec;
   k_copy_f32<<<g->num_sms * 4, 256, 0, s>>>(rhs, g->ppr_rhs, n);
-  k_copy_f32<<<g->num_sms * 4, 256, 0, s>>>(w, g->ppr_w, g->edges);
+  // the weights in the order the solve reads its adjacency (CSC order for the
+  // forward pull, so no edge-id indirection per edge and iteration)
+  if (dir == 0) k_gather_f32<<<g->num_sms * 4, 256, 0, s>>>(g->csr.csc_eid, w, g->ppr_w, g->edges);
+  else k_copy_f32<<<g->num_sms * 4, 256, 0, s>>>(w, g->ppr_w, g->edges);
   count_launch(2);
   w = g->ppr_w;
   rhs = g->ppr_rhs;
   PprArgs a;
   a.off = dir == 0 ? g->csr.csc_offsets : g->csr.row_offsets;
   a.idx = dir == 0 ? g->csr.csc_rows : g->csr.col;
-  a.eid = dir == 0 ? g->csr.csc_eid : nullptr;
+  a.eid = nullptr;
   a.w = w;
   a.rhs = rhs;
   a.alpha = alpha;
@@ -344,9 +359,10 @@ static int ppr_solve(mg_graph *g, int dir, const float *w, const float *rhs, flo
   k_copy_f32<<<g->num_sms * 4, 256, 0, s>>>(rhs, a.x0, n);
   const uint32_t max_iter = (uint32_t)std::max<int32_t>(0, std::min<int32_t>(o->iter_num, 100000));
   k_ctl_init<<<1, 32, 0, s>>>(a.ctl, 1u, max_iter, (unsigned long long)o->spin_limit, MODE_QUEUE, 0u);
-  count_launch(2);
+  k_ppr_rhs_norm<<<g->num_sms * 4, 256, 0, s>>>(rhs, n, a.ctl);
+  count_launch(3);
   const int grid = persistent_grid(g, o, 4);
-  const double tol_total = o->tolerance * (double)nvec;
+  const double tol = o->tolerance;
   const bool two = nvec > 32;
   LevelBody body = [=](cudaStream_t ss, cudaGraphConditionalHandle h, int use_h) {
     if (two) {
@@ -356,10 +372,10 @@ static int ppr_solve(mg_graph *g, int dir, const float *w, const float *rhs, flo
       MG_LAUNCH(KID_PPR, ss, k_ppr_iter<1><<<grid, kNT, 0, ss>>>(a));
       MG_LAUNCH(KID_PPR, ss, k_ppr_fixup<1><<<grid, kNT, 0, ss>>>(a));
     }
-    MG_LAUNCH(KID_OTHER, ss, k_ppr_level_end<<<1, 32, 0, ss>>>(a.ctl, tol_total, h, use_h));
+    MG_LAUNCH(KID_OTHER, ss, k_ppr_level_end<<<1, 32, 0, ss>>>(a.ctl, tol, h, use_h));
   };
   char key[160];
-  snprintf(key, sizeof(key), "%s/%d/%d/%.9g/%.17g/%.17g", name, grid, nvec, (double)alpha, o->damping, tol_total);
+  snprintf(key, sizeof(key), "%s/%d/%d/%.9g/%.17g/%.17g", name, grid, nvec, (double)alpha, o->damping, tol);
   int st = run_level_loop(g, s, key, 3, body, o->use_cuda_graph != 0, res);
   if (st != MG_OK) return st;
   finish_run(g, res->ctl.level);
@@ -369,7 +385,8 @@ static int ppr_solve(mg_graph *g, int dir, const float *w, const float *rhs, flo
   return MG_OK;
 }
 
-static void ppr_stats(mg_stats *stats, const LoopResult &res, double tol_total, mg_graph *g) {
+static void ppr_stats(mg_stats *stats, const LoopResult &res, double tol, mg_graph *g) {
+  const double tol_total = tol * res.ctl.acc[2];
   if (!stats) return;
   stats->iterations = (int32_t)res.ctl.level;
   stats->push_iterations = 0;
@@ -415,7 +432,7 @@ int mg_ppr_forward(mg_graph *g, const float *edge_weights, const float *teleport
   if ((st = ppr_solve(g, 0, edge_weights, teleport, (float)(1.0 - o->damping), nvec, o, s, "ppr_fwd", &x, &res)) !=
       MG_OK)
     return st;
-  ppr_stats(stats, res, o->tolerance * nvec, g);
+  ppr_stats(stats, res, o->tolerance, g);
   return copy_out(s, ranks, x, (size_t)g->nodes * nvec * 4, true);
 }
 
@@ -454,7 +471,7 @@ int mg_ppr_backward(mg_graph *g, const float *edge_weights, const float *ranks, 
                                                 (int64_t)g->nodes * nvec);
     count_launch();
   }
-  ppr_stats(stats, res, o->tolerance * nvec, g);
+  ppr_stats(stats, res, o->tolerance, g);
   return cuda_status(cudaStreamSynchronize(s), "ppr backward");
 }
 

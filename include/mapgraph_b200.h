@@ -196,7 +196,9 @@ int mg_pagerank_gas(mg_graph *g, float *ranks, mg_stats *stats, const mg_options
 
 /* Personalised PageRank with nvec teleport columns (device pointers, row-major
  * [nodes][nvec]): R = (1-d) T + d P^T R, P[u,v] = edge_weight[e(u,v)] (weights given
- * per CSR edge, already row-normalised by the caller). No reference counterpart. */
+ * per CSR edge, already row-normalised by the caller). No reference counterpart.
+ * Both solves iterate until the L1 change over all entries is <= tolerance times
+ * the L1 norm of their right-hand side (T here, dL/dR for the adjoint). */
 int mg_ppr_forward(mg_graph *g, const float *edge_weights, const float *teleport,
                    int32_t nvec, float *ranks, mg_stats *stats, const mg_options *opts);
 /* Adjoint of mg_ppr_forward: given the converged ranks and dL/dR, solves
