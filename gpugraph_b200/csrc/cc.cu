@@ -41,20 +41,22 @@ MG_DEVINL int32_t cc_find(int32_t *parent, int32_t x) {
   }
 }
 
-// Links the components of a and b (larger root under the smaller). A failed
-// compare-and-swap means another link changed a root first; the retries are
-// bounded and report failure instead of looping.
+// Links the components of a and b: the larger root is hooked under the smaller
+// with atomicMin, which always succeeds. If the larger one was no longer a
+// root (another link hooked it to `old` first), its tree and the smaller root
+// still have to be joined: link old with the smaller root next. Every round
+// hooks something, parent values only decrease, and the retries are bounded
+// all the same (a failure is reported, not looped on).
 MG_DEVINL bool cc_unite(int32_t *parent, int32_t a, int32_t b, unsigned long long limit) {
   for (unsigned long long it = 0; it < limit; ++it) {
     a = cc_find(parent, a);
     b = cc_find(parent, b);
     if (a == b) return true;
-    if (a < b) {
-      const int32_t t = a;
-      a = b;
-      b = t;
-    }
-    if (atomicCAS(&parent[a], a, b) == a) return true;
+    const int32_t hi = a > b ? a : b, lo = a > b ? b : a;
+    const int32_t old = atomicMin(&parent[hi], lo);
+    if (old == hi) return true;
+    a = old;
+    b = lo;
   }
   return false;
 }
@@ -107,20 +109,44 @@ __global__ void __launch_bounds__(kCcProbe) k_cc_giant(const int32_t *parent, in
   }
 }
 
-// Step 3: vertices outside the large component link their remaining edges.
+// Step 3: vertices outside the large component link their remaining edges. A
+// warp takes 32 consecutive vertices; lists up to 32 edges are walked by their
+// own lane, longer ones by the whole warp (32 edges per step).
 __global__ void __launch_bounds__(kNT) k_cc_rest(const int32_t *ro, const int32_t *col, int32_t *parent, int32_t V,
                                                  const int32_t *giant, Ctl *ctl) {
   const unsigned long long limit = ctl->spin_limit;
   const int32_t big = *giant;
+  const int lane = lane_id();
   bool ok = true;
   unsigned long long my_bytes = 0;
-  for (int v = blockIdx.x * blockDim.x + threadIdx.x; v < V; v += gridDim.x * blockDim.x) {
-    my_bytes += 12;  // parent, two offsets
-    if (__ldcg(&parent[v]) == big) continue;
-    const int end = ro[v + 1];
-    for (int e = ro[v] + kCcSample; e < end; ++e) {
-      my_bytes += 4;
-      if (!cc_unite(parent, v, col[e], limit)) ok = false;
+  const uint32_t groups = ((uint32_t)V + 31) / 32;
+  for (uint32_t grp = (blockIdx.x * blockDim.x + threadIdx.x) / 32; grp < groups;
+       grp += (gridDim.x * blockDim.x) / 32) {
+    const int v = (int)(grp * 32) + lane;
+    bool work = false;
+    int b = 0, e = 0;
+    if (v < V) {
+      my_bytes += 12;  // parent, two offsets
+      b = ro[v] + kCcSample;
+      e = ro[v + 1];
+      work = b < e && __ldcg(&parent[v]) != big;
+    }
+    if (work && e - b <= 32) {
+      for (int k = b; k < e; ++k) {
+        my_bytes += 4;
+        if (!cc_unite(parent, v, col[k], limit)) ok = false;
+      }
+    }
+    uint32_t heavy = __ballot_sync(0xffffffffu, work && e - b > 32);
+    while (heavy) {
+      const int h = __ffs(heavy) - 1;
+      heavy &= heavy - 1;
+      const int hv = (int)(grp * 32) + h;
+      const int hb = __shfl_sync(0xffffffffu, b, h), he = __shfl_sync(0xffffffffu, e, h);
+      for (int k = hb + lane; k < he; k += 32) {
+        my_bytes += 4;
+        if (!cc_unite(parent, hv, col[k], limit)) ok = false;
+      }
     }
   }
   if (!ok) raise_error(ctl, MG_ERR_TIMEOUT);
