@@ -98,6 +98,10 @@ struct mg_graph {
   int32_t pr_nchunks = 0, pr_nheavy = 0;
   int64_t pr_ndangling = 0;
   float *pr_rank[2] = {nullptr, nullptr}, *pr_contrib[2] = {nullptr, nullptr}, *pr_partial = nullptr;
+  // The in-lists the PageRank kernels read: on a skewed degree distribution a
+  // copy with vertices renumbered by descending out-degree (pr_new_of[v] = the
+  // new number of v), otherwise the graph's own CSC (pr_new_of null).
+  int32_t *pr_coff = nullptr, *pr_crow = nullptr, *pr_new_of = nullptr;
   // Personalised PageRank: chunk plans over the CSC (forward) and the CSR
   // (adjoint): chunk c covers edges [cb, ce) of vertex cv; cslot >= 0 marks a
   // partial of a split in-list, combined in chunk order by the fix-up pass.

@@ -39,6 +39,7 @@ constexpr int kPrChunk = 1024;  // edges per chunk of a long in-list
 constexpr int kPrGroup = 32;    // vertices per warp group (one per lane)
 constexpr int kPrSub = 4;       // 32-edge sub-chunks whose loads are in flight together
 constexpr int kPrSerial = 8;    // a group whose lists are all this short is summed lane by lane
+constexpr double kPrSkew = 64.0;  // renumber by out-degree when the largest is this many times the mean
 
 struct PrArgs {
   const int32_t *coff, *crow;
@@ -272,7 +273,28 @@ __global__ void k_pr_init(const float *inv, float *r, float *c, int32_t V, float
   }
 }
 
-// One-time plan: 1/outdeg, dangling count, heavy vertices and their chunks.
+// Renumbered in-lists: new vertex i is old vertex old_of[i]; its in-list is the
+// old in-list with every neighbour renumbered (order kept). Warp per vertex.
+__global__ void __launch_bounds__(kNT) k_pr_renumber(const int32_t *old_of, const int32_t *new_of,
+                                                     const int32_t *co, const int32_t *crow, const int32_t *coff_new,
+                                                     int32_t *crow_new, int32_t V) {
+  const int lane = lane_id();
+  for (int i = (blockIdx.x * blockDim.x + threadIdx.x) / 32; i < V; i += (gridDim.x * blockDim.x) / 32) {
+    const int v = old_of[i];
+    const int b = co[v], n = co[v + 1] - b, o = coff_new[i];
+    for (int k = lane; k < n; k += 32) crow_new[o + k] = new_of[crow[b + k]];
+  }
+}
+
+// ranks in the caller's numbering: out[v] = r[new_of[v]]
+__global__ void k_pr_unrenumber(const float *r, const int32_t *new_of, float *out, int32_t V) {
+  for (int v = blockIdx.x * blockDim.x + threadIdx.x; v < V; v += gridDim.x * blockDim.x) out[v] = r[new_of[v]];
+}
+
+// One-time plan: the in-lists to read (renumbered by descending out-degree when
+// the distribution is skewed, so the contributions of the most-gathered
+// vertices share cache lines), 1/outdeg, dangling count, heavy vertices and
+// their chunks.
 static int pr_plan(mg_graph *g, cudaStream_t s) {
   if (g->pr_rank[0]) return MG_OK;
   const int64_t V = g->nodes;
@@ -282,11 +304,54 @@ static int pr_plan(mg_graph *g, cudaStream_t s) {
   if (e == cudaSuccess) e = cudaMemcpyAsync(co.data(), g->csr.csc_offsets, (V + 1) * 4, cudaMemcpyDeviceToHost, s);
   if (e == cudaSuccess) e = cudaStreamSynchronize(s);
   if (e != cudaSuccess) return cuda_status(e, "pagerank plan read");
+  // Renumber when the out-degree distribution is skewed (a power law): the
+  // largest out-degree is many times the mean. Grid-like graphs keep their own
+  // numbering, whose locality is already good.
+  int32_t max_od = 0;
+  for (int64_t v = 0; v < V; ++v) max_od = std::max(max_od, ro[v + 1] - ro[v]);
+  const double mean_od = V ? (double)ro[V] / (double)V : 0.0;
+  const bool renumber = V > 0 && (double)max_od > kPrSkew * std::max(1.0, mean_od);
+  std::vector<int32_t> old_of, new_of;
+  if (renumber) {
+    old_of.resize((size_t)V);
+    new_of.resize((size_t)V);
+    for (int64_t v = 0; v < V; ++v) old_of[v] = (int32_t)v;
+    std::stable_sort(old_of.begin(), old_of.end(),
+                     [&](int32_t x, int32_t y) { return ro[x + 1] - ro[x] > ro[y + 1] - ro[y]; });
+    for (int64_t i = 0; i < V; ++i) new_of[old_of[i]] = (int32_t)i;
+    // offsets of the renumbered in-lists
+    std::vector<int32_t> cn((size_t)V + 1, 0);
+    for (int64_t i = 0; i < V; ++i) cn[i + 1] = cn[i] + (co[old_of[i] + 1] - co[old_of[i]]);
+    int st;
+    int32_t *d_old = nullptr, *d_new = nullptr, *d_cn = nullptr, *d_crow = nullptr;
+    if ((st = device_alloc(g, (void **)&d_old, (size_t)V * 4)) != MG_OK ||
+        (st = device_alloc(g, (void **)&d_new, (size_t)V * 4)) != MG_OK ||
+        (st = device_alloc(g, (void **)&d_cn, ((size_t)V + 1) * 4)) != MG_OK ||
+        (st = device_alloc(g, (void **)&d_crow, (size_t)g->edges * 4 + 64)) != MG_OK)
+      return st;
+    cudaError_t e2 = cudaMemcpyAsync(d_old, old_of.data(), (size_t)V * 4, cudaMemcpyHostToDevice, s);
+    if (e2 == cudaSuccess) e2 = cudaMemcpyAsync(d_new, new_of.data(), (size_t)V * 4, cudaMemcpyHostToDevice, s);
+    if (e2 == cudaSuccess) e2 = cudaMemcpyAsync(d_cn, cn.data(), ((size_t)V + 1) * 4, cudaMemcpyHostToDevice, s);
+    if (e2 != cudaSuccess) return cuda_status(e2, "pagerank renumbering upload");
+    k_pr_renumber<<<g->num_sms * 8, kNT, 0, s>>>(d_old, d_new, g->csr.csc_offsets, g->csr.csc_rows, d_cn, d_crow,
+                                                  (int32_t)V);
+    count_launch();
+    if ((st = launch_check("pagerank renumbering")) != MG_OK) return st;
+    g->pr_coff = d_cn;
+    g->pr_crow = d_crow;
+    g->pr_new_of = d_new;
+    co.swap(cn);  // the plan below is built on the renumbered in-lists
+  } else {
+    g->pr_coff = g->csr.csc_offsets;
+    g->pr_crow = g->csr.csc_rows;
+    g->pr_new_of = nullptr;
+  }
   std::vector<float> inv((size_t)V);
   int64_t ndang = 0;
   std::vector<int32_t> cv, cb, ce, hv, hf;
   for (int64_t v = 0; v < V; ++v) {
-    const int32_t od = ro[v + 1] - ro[v];
+    const int64_t ov = renumber ? old_of[v] : v;  // v in the numbering the kernels use
+    const int32_t od = ro[ov + 1] - ro[ov];
     inv[v] = od > 0 ? 1.0f / (float)od : 0.0f;
     ndang += od == 0;
     const int32_t b = co[v], en = co[v + 1];
@@ -360,8 +425,8 @@ extern "C" int mg_pagerank(mg_graph *g, float *ranks, mg_stats *stats, const mg_
   // the reference's iteration cap knob; the BASELINE specification stops at 100
   const uint32_t max_iter = (uint32_t)std::max<int32_t>(0, std::min<int32_t>(o->iter_num, 1 << 20));
   PrArgs a;
-  a.coff = g->csr.csc_offsets;
-  a.crow = g->csr.csc_rows;
+  a.coff = g->pr_coff;
+  a.crow = g->pr_crow;
   a.inv = g->inv_outdeg;
   a.r0 = g->pr_rank[0];
   a.r1 = g->pr_rank[1];
@@ -411,5 +476,13 @@ extern "C" int mg_pagerank(mg_graph *g, float *ranks, mg_stats *stats, const mg_
     stats->edges_traversed = g->edges * (int64_t)res.ctl.level;
   }
   const float *final_r = (res.ctl.level & 1) ? a.r1 : a.r0;
+  if (g->pr_new_of) {
+    // back to the caller's numbering, through the other rank buffer
+    float *out = (res.ctl.level & 1) ? a.r0 : a.r1;
+    k_pr_unrenumber<<<g->num_sms * 4, 256, 0, s>>>(final_r, g->pr_new_of, out, V);
+    count_launch();
+    if ((st = launch_check("pagerank renumbering")) != MG_OK) return st;
+    final_r = out;
+  }
   return copy_out(s, ranks, final_r, (size_t)V * 4, o->outputs_on_device != 0);
 }

@@ -218,3 +218,47 @@ def test_specialised_and_generic_engine_agree(generic):
     gr = Graph(road)
     d, _ = gr.sssp(77, generic_engine=generic)
     assert np.array_equal(d, oracle.sssp(road.row_offsets, road.column_indices, road.edge_values, 77))
+
+
+def test_new_paths_on_self_loops_duplicates_and_zero_weights():
+    # union-find CC, fused SSSP and predecessors on a hand-made symmetric graph with a
+    # self-loop, a duplicated edge, zero-weight edges, an isolated vertex and two components
+    edges = [(0, 1, 0), (1, 2, 5), (1, 2, 5), (2, 2, 3), (2, 3, 0), (4, 5, 7), (5, 6, 1), (3, 0, 2)]
+    n = 8  # vertex 7 isolated
+    sym = []
+    for u, v, w in edges:
+        sym.append((u, v, w))
+        if u != v:
+            sym.append((v, u, w))
+    sym.sort()
+    ro = np.zeros(n + 1, np.int32)
+    for u, _, _ in sym:
+        ro[u + 1] += 1
+    ro = np.cumsum(ro).astype(np.int32)
+    col = np.array([v for _, v, _ in sym], np.int32)
+    w = np.array([x for _, _, x in sym], np.int32)
+    hg = HostGraph(ro, col, w)
+    g = Graph(hg)
+    assert g.cc()[0].tolist() == oracle.cc(ro, col).tolist() == [0, 0, 0, 0, 4, 4, 4, 7]
+    for s in (0, 4, 7):
+        d, _ = g.sssp(s)
+        assert np.array_equal(d, oracle.sssp(ro, col, w, s)), s
+        dg, _ = g.sssp(s, generic_engine=1)
+        assert np.array_equal(dg, d)
+        depths, preds, _ = g.bfs_pred(s)
+        assert np.array_equal(depths, oracle.bfs(ro, col, s))
+        assert np.array_equal(preds, oracle.bfs_pred(ro, col, depths))
+    g.close()
+
+
+def test_cc_many_components_and_directed_program():
+    # many small components (a low edge factor leaves them) through union-find, and the
+    # directed push semantics through the GAS program on the same edges
+    hg = HostGraph.rmat(15, 1, seed=21)
+    g = Graph(hg)
+    labels, _ = g.cc()
+    ref = oracle.cc(hg.row_offsets, hg.column_indices)
+    assert np.array_equal(labels, ref) and len(np.unique(ref)) > 1000
+    dg = Graph(HostGraph.rmat(13, 4, seed=22, symmetrize=False), directed=True)
+    h2 = dg.host
+    assert np.array_equal(dg.cc()[0], oracle.cc(h2.row_offsets, h2.column_indices, "push"))
