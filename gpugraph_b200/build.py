@@ -76,8 +76,10 @@ def build(verbose_ptxas: bool = False, jobs: int | None = None) -> Path:
     with cf.ThreadPoolExecutor(max_workers=jobs or min(16, os.cpu_count() or 4)) as ex:
         objs = list(ex.map(lambda s: _compile(s, verbose_ptxas), srcs))
     tmp = LIB.with_suffix(".so.tmp")
+    # --no-undefined: a kernel stub declared in one file and renamed in another
+    # fails the build instead of the first dlopen
     cmd = [nvcc()] + ARCH + ["-shared", "-cudart", "static", "-o", str(tmp)] + [str(o) for o in objs] + [
-        "-Xcompiler", "-pthread"]
+        "-Xcompiler", "-pthread", "-Xlinker", "--no-undefined", "-lrt", "-ldl"]
     res = subprocess.run(cmd, capture_output=True, text=True)
     if res.returncode != 0:
         raise RuntimeError(f"link failed: {' '.join(cmd)}\n{res.stdout}\n{res.stderr}")

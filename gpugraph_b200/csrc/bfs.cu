@@ -381,13 +381,19 @@ __global__ void k_bfs_level_end(Ctl *ctl, int32_t V, int64_t E, cudaGraphConditi
   if (use_handle) cudaGraphSetConditional(h, ctl->active);
 }
 
-__global__ void k_bfs_init(Ctl *ctl, const int32_t *srcs, int32_t nsrc, int32_t *labels, uint32_t *visited,
-                           uint32_t *bm0, const int32_t *ro, uint32_t dir_policy, float alpha, float beta) {
+// Level-0 state. The roots are already in queue0, or (queue0_ready == 0, one
+// root) passed by value and written there here.
+__global__ void k_bfs_init(Ctl *ctl, int32_t *queue0, int queue0_ready, int32_t root, int32_t nsrc, int32_t *labels,
+                           uint32_t *visited, uint32_t *bm0, const int32_t *ro, uint32_t dir_policy, float alpha,
+                           float beta) {
   __shared__ unsigned long long s_edges;
-  if (threadIdx.x == 0) s_edges = 0;
+  if (threadIdx.x == 0) {
+    s_edges = 0;
+    if (!queue0_ready) queue0[0] = root;
+  }
   __syncthreads();
   for (int i = threadIdx.x; i < nsrc; i += blockDim.x) {
-    const int v = srcs[i];
+    const int v = queue0_ready ? queue0[i] : root;
     labels[v] = 0;
     atomicOr(&visited[v >> 5], 1u << (v & 31));
     atomicOr(&bm0[v >> 5], 1u << (v & 31));
@@ -414,11 +420,9 @@ int bfs_run(mg_graph *g, const std::vector<int32_t> &roots, int32_t *depths, mg_
     mg_options_init(&dflt);
     o = &dflt;
   }
-  if (o->direction == MG_DIR_PULL || o->direction == MG_DIR_AUTO) {
-    // Pull needs in-edges; they exist for every graph (CSC or the symmetric CSR).
-  } else if (o->direction != MG_DIR_PUSH) {
+  // (pull needs in-edges; every graph has them: its CSC or the symmetric CSR)
+  if (o->direction != MG_DIR_PULL && o->direction != MG_DIR_AUTO && o->direction != MG_DIR_PUSH)
     return set_error(MG_ERR_ARG, "unknown direction policy");
-  }
   cudaStream_t s = run_stream(g, o);
   int st = ensure_workspace(g);
   if (st != MG_OK) return st;
@@ -450,7 +454,10 @@ int bfs_run(mg_graph *g, const std::vector<int32_t> &roots, int32_t *depths, mg_
   // Every level of a traversal settles at least one vertex, so V + 2 levels bound
   // the device loop even if a Program never empties its frontier.
   const uint32_t max_iter = (uint32_t)std::min<int64_t>(o->iter_num > 0 ? o->iter_num : 0, g->nodes + 2);
-  cudaError_t e = cudaMemcpyAsync(w.queue[0], roots.data(), nsrc * 4, cudaMemcpyHostToDevice, s);
+  // one root goes to the init kernel by value; several are copied
+  const int queue0_ready = nsrc > 1 ? 1 : 0;
+  cudaError_t e = queue0_ready ? cudaMemcpyAsync(w.queue[0], roots.data(), nsrc * 4, cudaMemcpyHostToDevice, s)
+                               : cudaSuccess;
   if (e == cudaSuccess) e = cudaMemsetAsync(w.visited, 0, w.words * 4, s);
   if (e == cudaSuccess) e = cudaMemsetAsync(w.bm[0], 0, w.words * 4, s);
   if (e == cudaSuccess) e = cudaMemsetAsync(w.bm[1], 0, w.words * 4, s);
@@ -462,8 +469,8 @@ int bfs_run(mg_graph *g, const std::vector<int32_t> &roots, int32_t *depths, mg_
   const int push_grid = std::max(grid, g->num_sms * 6);
   k_fill_i32<<<g->num_sms * 4, 256, 0, s>>>(w.vbuf[0], BfsP::INIT_VALUE, V);
   k_ctl_init<<<1, 32, 0, s>>>(w.ctl, nsrc, max_iter, (unsigned long long)o->spin_limit, MODE_QUEUE, ctl_flags(o));
-  k_bfs_init<<<1, 256, 0, s>>>(w.ctl, w.queue[0], (int32_t)nsrc, w.vbuf[0], w.visited, w.bm[0], g->csr.row_offsets,
-                               (uint32_t)o->direction, (float)o->alpha, (float)o->beta);
+  k_bfs_init<<<1, 256, 0, s>>>(w.ctl, w.queue[0], queue0_ready, roots[0], (int32_t)nsrc, w.vbuf[0], w.visited, w.bm[0],
+                               g->csr.row_offsets, (uint32_t)o->direction, (float)o->alpha, (float)o->beta);
   count_launch(3);
   if ((st = launch_check("bfs init kernels")) != MG_OK) return st;
   const int32_t Vv = g->csr.V;
@@ -483,8 +490,15 @@ int bfs_run(mg_graph *g, const std::vector<int32_t> &roots, int32_t *depths, mg_
     MG_LAUNCH(KID_OTHER, ss, k_bfs_level_end<<<1, 32, 0, ss>>>(a.ctl, Vv, E, h, use_h));
   };
   LoopResult res;
+  // device output without predecessors: the depths are copied before the
+  // control block is read back (one host synchronisation)
+  const bool early_copy = o->outputs_on_device != 0 && !preds && depths;
+  int32_t *labels = w.vbuf[0];
+  const std::function<void(cudaStream_t)> epi = [=](cudaStream_t ss) {
+    cudaMemcpyAsync(depths, labels, (size_t)V * 4, cudaMemcpyDeviceToDevice, ss);
+  };
   st = run_level_loop(g, s, "bfs/" + std::to_string(grid) + (small_tiles ? "/t1024" : "/t2048"), 5, body,
-                      o->use_cuda_graph != 0, &res);
+                      o->use_cuda_graph != 0, &res, early_copy ? &epi : nullptr);
   if (st != MG_OK) return st;
   finish_run(g, res.ctl.level);
   if (res.ctl.error) return set_error(res.ctl.error, "bfs: device reported " + std::string(mg_status_string(res.ctl.error)));
@@ -509,6 +523,7 @@ int bfs_run(mg_graph *g, const std::vector<int32_t> &roots, int32_t *depths, mg_
     if ((st = launch_check("bfs predecessors")) != MG_OK) return st;
     if ((st = copy_out(s, preds, w.vbuf[1], (size_t)V * 4, o->outputs_on_device != 0)) != MG_OK) return st;
   }
+  if (early_copy) return MG_OK;
   return copy_out(s, depths, w.vbuf[0], (size_t)V * 4, o->outputs_on_device != 0);
 }
 

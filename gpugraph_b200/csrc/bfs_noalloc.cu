@@ -59,8 +59,9 @@ using NaP = programs::bfs;
 
 // Kernels defined with the rest of the BFS path (bfs.cu).
 __global__ void k_bfs_level_end(Ctl *ctl, int32_t V, int64_t E, cudaGraphConditionalHandle h, int use_handle);
-__global__ void k_bfs_init(Ctl *ctl, const int32_t *srcs, int32_t nsrc, int32_t *labels, uint32_t *visited,
-                           uint32_t *bm0, const int32_t *ro, uint32_t dir_policy, float alpha, float beta);
+__global__ void k_bfs_init(Ctl *ctl, int32_t *queue0, int queue0_ready, int32_t root, int32_t nsrc, int32_t *labels,
+                           uint32_t *visited, uint32_t *bm0, const int32_t *ro, uint32_t dir_policy, float alpha,
+                           float beta);
 
 namespace {
 constexpr int kNaMaxDevices = 64;
@@ -124,7 +125,6 @@ extern "C" int mg_bfs_noalloc(const int32_t *d_row_offsets, const int32_t *d_col
   if (e == cudaSuccess) e = cudaMemsetAsync(bm0, 0, words * 4, s);
   if (e == cudaSuccess) e = cudaMemsetAsync(bm1, 0, words * 4, s);
   if (e == cudaSuccess) e = cudaMemsetAsync(changed, 0, (size_t)nodes, s);
-  if (e == cudaSuccess) e = cudaMemcpyAsync(q0, &src, 4, cudaMemcpyHostToDevice, s);
   if (e != cudaSuccess) return cuda_status(e, "mg_bfs_noalloc: init");
 
   GasArgs<NaP> a;
@@ -159,7 +159,8 @@ extern "C" int mg_bfs_noalloc(const int32_t *d_row_offsets, const int32_t *d_col
   const uint32_t max_iter = (uint32_t)nodes + 2;
   k_fill_i32<<<sms * 4, 256, 0, s>>>(d_depths, NaP::INIT_VALUE, nodes);
   k_ctl_init<<<1, 32, 0, s>>>(ctl, 1u, max_iter, 1ull << 22, MODE_QUEUE, 0u);
-  k_bfs_init<<<1, 256, 0, s>>>(ctl, q0, 1, d_depths, visited, bm0, d_row_offsets, (uint32_t)MG_DIR_PUSH, 15.f, 18.f);
+  k_bfs_init<<<1, 256, 0, s>>>(ctl, q0, 0, src, 1, d_depths, visited, bm0, d_row_offsets, (uint32_t)MG_DIR_PUSH, 15.f,
+                               18.f);
   count_launch(3);
   if ((e = cudaGetLastError()) != cudaSuccess) return cuda_status(e, "mg_bfs_noalloc: init kernels");
   Ctl hc;
