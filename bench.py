@@ -157,7 +157,7 @@ def run_native(args, rank: int, world: int):
     import torch
 
     import gpugraph_b200 as gg
-    from gpugraph_b200 import _lib
+    from gpugraph_b200 import _lib, replicas
 
     lib = _lib.lib
     torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
@@ -191,8 +191,7 @@ def run_native(args, rank: int, world: int):
     lib.mg_kernel_launches(1)
     ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     with ClockSampler(torch.cuda.current_device()) as clk:
-        if world > 1:
-            torch.distributed.barrier()
+        replicas.barrier()
         torch.cuda.synchronize()
         h0 = time.time()
         ev0.record(stream)
@@ -201,15 +200,12 @@ def run_native(args, rank: int, world: int):
         ev1.record(stream)
         torch.cuda.synchronize()
         clk.mark(h0, time.time())
-        if world > 1:
-            torch.distributed.barrier()
+        replicas.barrier()
     launches = int(lib.mg_kernel_launches(1))
-    ms_step = ev0.elapsed_time(ev1) / args.steps
-    if world > 1:
-        t = torch.tensor([ms_step], device=dev)
-        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-        ms_step = float(t.item())
-    value = world * teps_edges / (ms_step * 1e-3) / 1e9
+    # N replicas: the units every rank processed over the slowest rank's device time
+    rate, step_s = replicas.aggregate_rate(teps_edges, ev0.elapsed_time(ev1) / args.steps * 1e-3, str(dev))
+    ms_step = step_s * 1e3
+    value = rate / 1e9
 
     # ---- plain engine: the same sources one at a time
     o_single = _lib.default_options(**base_opts)
@@ -284,11 +280,14 @@ def run_native(args, rank: int, world: int):
     _lib.check(lib.mg_bfs_multi(g.handle, src_pinned.data_ptr(), NSRC, host_out.data_ptr(), None, o_host), "e2e")
     torch.cuda.synchronize()
     e2e_steps = max(1, min(args.steps, 5))
-    t1 = time.perf_counter()
+    replicas.barrier()
+    ev0.record(stream)
     for _ in range(e2e_steps):
         _lib.check(lib.mg_bfs_multi(g.handle, src_pinned.data_ptr(), NSRC, host_out.data_ptr(), None, o_host), "e2e")
-    e2e_s = (time.perf_counter() - t1) / e2e_steps
-    e2e = {"value": world * teps_edges / e2e_s / 1e9, "unit": "GTEPS", "h2d_bytes_per_step": NSRC * 4,
+    ev1.record(stream)
+    torch.cuda.synchronize()
+    e2e_rate, e2e_s = replicas.aggregate_rate(teps_edges, ev0.elapsed_time(ev1) / e2e_steps * 1e-3, str(dev))
+    e2e = {"value": e2e_rate / 1e9, "unit": "GTEPS", "h2d_bytes_per_step": NSRC * 4,
            "d2h_bytes_per_step": NSRC * hg.nodes * 4, "ms_per_step": e2e_s * 1e3}
 
     # ---- live roofline of the dominant kernel (profiled pass, host-driven loop)
