@@ -1,7 +1,8 @@
-// Direction-optimising BFS (north_star (c)): push levels run the GAS engine
-// with the bfs Program (Algorithms/BFS/bfs.h:28-298) over a vertex queue; pull
-// levels run a bottom-up sweep in which every unvisited vertex scans its
-// in-edges for a parent in the frontier bitmap and stops at the first hit.
+// Direction-optimising BFS (north_star (c)): push levels run the bfs Program's
+// expand + contract (Algorithms/BFS/bfs.h:28-298) fused into k_bfs_push over a
+// vertex queue; pull levels run a bottom-up sweep in which every unvisited
+// vertex scans its in-edges (hubs first) for a parent in the frontier bitmap
+// and stops at the first hit.
 // The switch follows Beamer's rule: push -> pull when the next frontier's
 // out-edges exceed (unvisited edges)/alpha, pull -> push when the frontier
 // shrinks below nodes/beta. Depths are unique, so every schedule gives the

@@ -2,15 +2,16 @@
 // GASengine/csr_problem.cuh:150-354) and its working set.
 //
 // HBM layout, all int32 unless noted, every array 256-byte aligned:
-//   row_offsets[V+1+pad]  CSR offsets (padded to a multiple of 4 entries + 4 so
-//                         16-byte bulk copies of any aligned 4-entry tile stay in bounds)
+//   row_offsets[V+1+pad]  CSR offsets (padded with E to a multiple of 4 entries + 4,
+//                         so 16-byte reads of any aligned 4-entry piece stay in bounds)
 //   col[E+pad]            CSR column indices
 //   wgt[E]                int32 edge values (SSSP weights), optional
 //   csc_offsets/csc_rows  transposed graph (in-edges); aliases the CSR when the
 //                         graph is symmetric
 //   csc_eid[E]            CSR edge id of every CSC entry (pull access to edge values)
 //   pull_rows[E]          the in-lists again, hubs first (bottom-up BFS only)
-//   out_degree_inv[V]     float 1/outdeg (PageRank), built on first use
+//   inv_outdeg[V]         float 1/outdeg (PageRank), built on first use with the
+//                         PageRank plan (renumbered in-lists on skewed graphs)
 // The working set (queues, scan buffers, bitmaps, look-back status words) is
 // allocated once per graph and reused by every run on it.
 #pragma once
