@@ -110,3 +110,64 @@ def test_graph_batch_bfs():
         assert np.array_equal(out[b:e], oracle.bfs(h.row_offsets, h.column_indices, local[i])), i
     with pytest.raises(MapGraphError):
         g.bfs_batch(np.full(24, 1 << 20, np.int32))
+
+
+def test_multi_isolated_sources_and_edge_free_graph():
+    # sources with no out-edges finish at level 0 while the others keep expanding; an
+    # edge-free graph ends after the first level for every source
+    hg = HostGraph.rmat(12, 4, seed=31).with_weights(1, 50, seed=31)
+    iso = np.flatnonzero(hg.out_degree() == 0)
+    assert iso.size >= 8
+    srcs = np.concatenate([iso[:8], seeded_sources(hg, 56, seed=9)]).astype(np.int32)
+    g = Graph(hg)
+    ref = np.stack([oracle.bfs(hg.row_offsets, hg.column_indices, s) for s in srcs])
+    for d in DIRS:
+        assert np.array_equal(g.bfs_multi(srcs, direction=d)[0], ref), d
+    out, _ = g.sssp_multi(srcs)
+    for k in (0, 7, 8, 63):
+        assert np.array_equal(out[k], oracle.sssp(hg.row_offsets, hg.column_indices, hg.edge_values, srcs[k])), k
+    for k in range(8):
+        assert (out[k] == SSSP_INF).sum() == hg.nodes - 1 and out[k][srcs[k]] == 0
+    n = 300
+    empty = HostGraph(np.zeros(n + 1, np.int32), np.zeros(0, np.int32), np.zeros(0, np.int32))
+    ge = Graph(empty)
+    s = np.array([0, 299, 5, 5], np.int32)
+    bo, _ = ge.bfs_multi(s)
+    so, _ = ge.sssp_multi(s)
+    for k, v in enumerate(s):
+        exp = np.full(n, -1, np.int32)
+        exp[v] = 0
+        assert np.array_equal(bo[k], exp)
+        exp_s = np.full(n, SSSP_INF, np.int32)
+        exp_s[v] = 0
+        assert np.array_equal(so[k], exp_s)
+
+
+@pytest.mark.parametrize("nsrc", [64, 20])
+def test_sssp_multi_directed_duplicates_zero_weights(nsrc):
+    # 64 sources run the dense relaxation mode, 20 the sparse one; duplicated sources and
+    # zero-weight edges must give each row the single-source distances
+    hg = HostGraph.rmat(12, 8, seed=41, symmetrize=False).with_weights(0, 9, seed=41)
+    assert (hg.edge_values == 0).any()
+    g = Graph(hg, directed=True)
+    base = seeded_sources(hg, nsrc - 4, seed=5)
+    srcs = np.concatenate([base, base[:4]]).astype(np.int32)
+    out, _ = g.sssp_multi(srcs)
+    for k, s in enumerate(srcs):
+        assert np.array_equal(out[k], oracle.sssp(hg.row_offsets, hg.column_indices, hg.edge_values, s)), k
+    assert np.array_equal(out[:4], out[nsrc - 4:])
+
+
+def test_graph_batch_with_trivial_graphs():
+    # single-vertex, edge-free and path graphs mixed with R-MAT graphs in one batch
+    one = HostGraph(np.array([0, 0], np.int32), np.zeros(0, np.int32))
+    bare = HostGraph(np.zeros(6, np.int32), np.zeros(0, np.int32))
+    path = HostGraph(np.array([0, 1, 3, 5, 6], np.int32), np.array([1, 0, 2, 1, 3, 2], np.int32))
+    graphs = [one, HostGraph.rmat(9, 8, seed=3), bare, path, one, HostGraph.rmat(7, 4, seed=4), path]
+    big = concat_graphs(graphs)
+    g = Graph(big)
+    local = np.array([0, graphs[1].max_degree_vertex(), 4, 0, 0, 3, 2], np.int32)
+    out, _ = g.bfs_batch(local)
+    for i, h in enumerate(graphs):
+        b, e = big.graph_offsets[i], big.graph_offsets[i + 1]
+        assert np.array_equal(out[b:e], oracle.bfs(h.row_offsets, h.column_indices, local[i])), i
