@@ -412,6 +412,39 @@ __global__ void k_bfs_init(Ctl *ctl, int32_t *queue0, int queue0_ready, int32_t 
   }
 }
 
+// Level-0 state of a single-root BFS in one launch (instead of clearing the
+// three bitmaps, filling the depths, and initialising the control block and
+// the root separately): every depth and bitmap word is written once, the
+// root's with its level-0 value.
+__global__ void k_bfs_start(Ctl *ctl, int32_t *queue0, int32_t root, int32_t *labels, uint32_t *visited, uint32_t *bm0,
+                            uint32_t *bm1, int32_t V, const int32_t *ro, uint32_t max_iter,
+                            unsigned long long spin_limit, uint32_t flags, uint32_t dir_policy, float alpha,
+                            float beta) {
+  const int64_t words = ((int64_t)V + 31) / 32;
+  const int64_t rw = root >> 5;
+  const uint32_t rb = 1u << (root & 31);
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < V; i += (int64_t)gridDim.x * blockDim.x) {
+    labels[i] = (i == root) ? 0 : BfsP::INIT_VALUE;
+    if (i < words) {
+      const uint32_t x = (i == rw) ? rb : 0u;
+      visited[i] = x;
+      bm0[i] = x;
+      bm1[i] = 0u;
+    }
+  }
+  if (blockIdx.x == 0 && threadIdx.x == 0) {
+    ctl_init_body(ctl, 1u, max_iter, spin_limit, MODE_QUEUE, flags);
+    queue0[0] = root;
+    ctl->visited_edges = (unsigned long long)(ro[root + 1] - ro[root]);
+    ctl->visited_count = 1;
+    ctl->dir_policy = dir_policy;
+    ctl->alpha = alpha;
+    ctl->beta = beta;
+    ctl->mode = (dir_policy == MG_DIR_PULL) ? MODE_BITMAP : MODE_QUEUE;
+    ctl->convert = 0;
+  }
+}
+
 // Shared by mg_bfs, mg_bfs_roots and mg_bfs_batch.
 // `preds` (optional): predecessors by the pred_extract rule (k_bfs_pred).
 int bfs_run(mg_graph *g, const std::vector<int32_t> &roots, int32_t *depths, mg_stats *stats, const mg_options *o,
@@ -457,22 +490,31 @@ int bfs_run(mg_graph *g, const std::vector<int32_t> &roots, int32_t *depths, mg_
   const uint32_t max_iter = (uint32_t)std::min<int64_t>(o->iter_num > 0 ? o->iter_num : 0, g->nodes + 2);
   // one root goes to the init kernel by value; several are copied
   const int queue0_ready = nsrc > 1 ? 1 : 0;
-  cudaError_t e = queue0_ready ? cudaMemcpyAsync(w.queue[0], roots.data(), nsrc * 4, cudaMemcpyHostToDevice, s)
-                               : cudaSuccess;
-  if (e == cudaSuccess) e = cudaMemsetAsync(w.visited, 0, w.words * 4, s);
-  if (e == cudaSuccess) e = cudaMemsetAsync(w.bm[0], 0, w.words * 4, s);
-  if (e == cudaSuccess) e = cudaMemsetAsync(w.bm[1], 0, w.words * 4, s);
-  if ((st = cuda_status(e, "bfs init")) != MG_OK) return st;
+  if (queue0_ready) {
+    cudaError_t e = cudaMemcpyAsync(w.queue[0], roots.data(), nsrc * 4, cudaMemcpyHostToDevice, s);
+    if (e == cudaSuccess) e = cudaMemsetAsync(w.visited, 0, w.words * 4, s);
+    if (e == cudaSuccess) e = cudaMemsetAsync(w.bm[0], 0, w.words * 4, s);
+    if (e == cudaSuccess) e = cudaMemsetAsync(w.bm[1], 0, w.words * 4, s);
+    if ((st = cuda_status(e, "bfs init")) != MG_OK) return st;
+  }
   const int grid = persistent_grid(g, o, 4);
   // the pull kernel holds no shared memory and at most 40 registers: 48 warps per SM
   const int pull_grid = g->num_sms * 6;
   // the push kernel: at most 40 registers and 25 KB of shared memory, 6 CTAs per SM
   const int push_grid = std::max(grid, g->num_sms * 6);
-  k_fill_i32<<<g->num_sms * 4, 256, 0, s>>>(w.vbuf[0], BfsP::INIT_VALUE, V);
-  k_ctl_init<<<1, 32, 0, s>>>(w.ctl, nsrc, max_iter, (unsigned long long)o->spin_limit, MODE_QUEUE, ctl_flags(o));
-  k_bfs_init<<<1, 256, 0, s>>>(w.ctl, w.queue[0], queue0_ready, roots[0], (int32_t)nsrc, w.vbuf[0], w.visited, w.bm[0],
-                               g->csr.row_offsets, (uint32_t)o->direction, (float)o->alpha, (float)o->beta);
-  count_launch(3);
+  if (queue0_ready) {
+    k_fill_i32<<<g->num_sms * 4, 256, 0, s>>>(w.vbuf[0], BfsP::INIT_VALUE, V);
+    k_ctl_init<<<1, 32, 0, s>>>(w.ctl, nsrc, max_iter, (unsigned long long)o->spin_limit, MODE_QUEUE, ctl_flags(o));
+    k_bfs_init<<<1, 256, 0, s>>>(w.ctl, w.queue[0], queue0_ready, roots[0], (int32_t)nsrc, w.vbuf[0], w.visited,
+                                 w.bm[0], g->csr.row_offsets, (uint32_t)o->direction, (float)o->alpha, (float)o->beta);
+    count_launch(3);
+  } else {
+    k_bfs_start<<<g->num_sms * 4, 256, 0, s>>>(w.ctl, w.queue[0], roots[0], w.vbuf[0], w.visited, w.bm[0], w.bm[1], V,
+                                               g->csr.row_offsets, max_iter, (unsigned long long)o->spin_limit,
+                                               ctl_flags(o), (uint32_t)o->direction, (float)o->alpha,
+                                               (float)o->beta);
+    count_launch(1);
+  }
   if ((st = launch_check("bfs init kernels")) != MG_OK) return st;
   const int32_t Vv = g->csr.V;
   const int64_t E = g->edges;

@@ -509,9 +509,8 @@ static __global__ void k_sequence_i32(int32_t *p, int64_t n) {
 }
 
 // flags: bit 0 = ordered frontier compaction (mg_options.ordered_frontier)
-static __global__ void k_ctl_init(Ctl *ctl, uint32_t frontier_size, uint32_t max_iter, unsigned long long spin_limit,
-                           uint32_t mode, uint32_t flags) {
-  if (threadIdx.x != 0) return;
+MG_DEVINL void ctl_init_body(Ctl *ctl, uint32_t frontier_size, uint32_t max_iter, unsigned long long spin_limit,
+                             uint32_t mode, uint32_t flags) {
   // The epoch keeps growing across runs so stale look-back words never match;
   // the host zeroes the status words and the control block before the 30-bit
   // field could wrap (see prepare_run).
@@ -527,6 +526,11 @@ static __global__ void k_ctl_init(Ctl *ctl, uint32_t frontier_size, uint32_t max
   c.active = (frontier_size > 0 && max_iter > 0) ? 1u : 0u;
   c.ordered = flags & 1u;
   *ctl = c;
+}
+
+static __global__ void k_ctl_init(Ctl *ctl, uint32_t frontier_size, uint32_t max_iter, unsigned long long spin_limit,
+                                  uint32_t mode, uint32_t flags) {
+  if (threadIdx.x == 0) ctl_init_body(ctl, frontier_size, max_iter, spin_limit, mode, flags);
 }
 
 inline uint32_t ctl_flags(const mg_options *o) { return (o && o->ordered_frontier) ? 1u : 0u; }
