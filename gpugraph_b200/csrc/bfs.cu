@@ -4,8 +4,8 @@
 // vertex scans its in-edges (hubs first) for a parent in the frontier bitmap
 // and stops at the first hit.
 // The switch follows Beamer's rule: push -> pull when the next frontier's
-// out-edges exceed (unvisited edges)/alpha, pull -> push when the frontier
-// shrinks below nodes/beta. Depths are unique, so every schedule gives the
+// out-edges exceed (unvisited edges)/alpha while the frontier grows, pull ->
+// push when the frontier shrinks below nodes/beta. Depths are unique, so every schedule gives the
 // same labels as the reference's CPUBFS (Algorithms/BFS/bfs.cu:57-111).
 #include <cuda_runtime.h>
 
@@ -45,14 +45,14 @@ __global__ void __launch_bounds__(kNT, 6) k_bfs_pull(GasArgs<BfsP> a) {
   const int32_t *coff = a.g.csc_offsets, *crow = a.g.pull_rows, *ro = a.g.row_offsets;
   const int lane = lane_id();
   unsigned long long my_cnt = 0, my_edges = 0, my_bytes = 0;
-  // tickets (kPullWords words each) are handed out dynamically; the next one
-  // is drawn while the current one is processed
-  uint32_t ticket = 0;
-  if (lane == 0) ticket = atomicAdd(&ctl->group_ctr, 1u);
-  for (;;) {
-    const uint32_t t = __shfl_sync(0xffffffffu, ticket, 0);
-    if (t >= tickets) break;
-    if (lane == 0) ticket = atomicAdd(&ctl->group_ctr, 1u);
+  __shared__ unsigned long long s_tot[2];
+  if (threadIdx.x < 2) s_tot[threadIdx.x] = 0;
+  __syncthreads();
+  // Tickets (kPullWords words each) are dealt round-robin over the grid's
+  // warps: one atomic per ticket on a shared counter costs more than the
+  // imbalance it would remove (measured on R-MAT 22: 317 vs 342 us per BFS).
+  const uint32_t nwarps = (gridDim.x * blockDim.x) >> 5;
+  for (uint32_t t = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; t < tickets; t += nwarps) {
     uint32_t vis[kPullWords];
     int beg[kPullWords], end[kPullWords];
 #pragma unroll
@@ -124,11 +124,14 @@ __global__ void __launch_bounds__(kNT, 6) k_bfs_pull(GasArgs<BfsP> a) {
       }
     }
   }
-  add_bytes(ctl->kbytes, KID_BFS_PULL, my_bytes);
-  // per-warp totals straight to the control block (no block barrier at the end)
+  add_bytes(ctl, KID_BFS_PULL, my_bytes);
+  // totals per CTA, then one atomic per CTA and counter on the control block
   my_edges = warp_sum(my_edges);
-  if (lane == 0 && my_cnt) atomicAdd((unsigned long long *)&ctl->acc[0], my_cnt);
-  if (lane == 0 && my_edges) atomicAdd(&ctl->next_edges, my_edges);
+  if (lane == 0 && my_cnt) atomicAdd(&s_tot[0], my_cnt);
+  if (lane == 0 && my_edges) atomicAdd(&s_tot[1], my_edges);
+  __syncthreads();
+  if (threadIdx.x == 0 && s_tot[0]) atomicAdd((unsigned long long *)&ctl->acc[0], s_tot[0]);
+  if (threadIdx.x == 0 && s_tot[1]) atomicAdd(&ctl->next_edges, s_tot[1]);
 }
 
 // Top-down level of the bfs program (the engine's expand + contract with the
@@ -226,7 +229,7 @@ __global__ void __launch_bounds__(kNT, 6) k_bfs_push(GasArgs<BfsP> a) {
                           Fout, (uint32_t)V, ctl))
       break;
   }
-  add_bytes(ctl->kbytes, KID_EXPAND, my_bytes);
+  add_bytes(ctl, KID_EXPAND, my_bytes);
   my_edges = warp_sum(my_edges);
   if (lane == 0 && my_edges) atomicAdd(&s_edges, my_edges);
   __syncthreads();
@@ -362,7 +365,10 @@ __global__ void k_bfs_level_end(Ctl *ctl, int32_t V, int64_t E, cudaGraphConditi
       new_mode = MODE_BITMAP;
     } else if (mode == MODE_QUEUE) {
       const double unvisited_edges = (double)E - (double)ctl->visited_edges;
-      if ((double)m_next > unvisited_edges / (double)ctl->alpha) new_mode = MODE_BITMAP;
+      // only while the frontier grows: near the end of a search the unvisited
+      // edges are few, and a sweep over every vertex costs more than the push
+      if ((double)m_next > unvisited_edges / (double)ctl->alpha && n_next > ctl->frontier_size)
+        new_mode = MODE_BITMAP;
     } else {
       if ((double)n_next < (double)V / (double)ctl->beta && n_next < ctl->frontier_size) new_mode = MODE_QUEUE;
     }

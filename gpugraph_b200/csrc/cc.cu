@@ -150,7 +150,7 @@ __global__ void __launch_bounds__(kNT) k_cc_rest(const int32_t *ro, const int32_
     }
   }
   if (!ok) raise_error(ctl, MG_ERR_TIMEOUT);
-  add_bytes(ctl->kbytes, KID_OTHER, my_bytes);
+  add_bytes(ctl, KID_OTHER, my_bytes);
 }
 
 // Final labels: every vertex's root (the smallest id of its component).
@@ -175,7 +175,7 @@ int cc_union_find(mg_graph *g, int32_t *labels, mg_stats *stats, const mg_option
   int32_t *giant = reinterpret_cast<int32_t *>(g->ws.scan);  // scratch word (the scan buffer is free here)
   const int vgrid = g->num_sms * 8;
   k_sequence_i32<<<g->num_sms * 4, 256, 0, s>>>(parent, V);
-  k_ctl_init<<<1, 32, 0, s>>>(ctl, 1u, 1u, (unsigned long long)o->spin_limit, MODE_QUEUE, 0u);
+  k_ctl_init<<<1, 32, 0, s>>>(ctl, 1u, 1u, (unsigned long long)o->spin_limit, MODE_QUEUE, ctl_flags(nullptr));
   for (int r = 0; r < kCcSample; ++r) {
     k_cc_sample<<<vgrid, kNT, 0, s>>>(g->csr.row_offsets, g->csr.col, parent, V, r, ctl);
     k_cc_flatten<<<vgrid, kNT, 0, s>>>(parent, V);

@@ -43,6 +43,7 @@ struct Ctl {
   uint32_t group_ctr;       // dynamic work counter of the pull kernels
   uint32_t prev_size;       // |F| of the previous level (batched traversals)
   uint32_t apply_pending;   // 1: the previous push level left bits to apply
+  uint32_t count_bytes;     // 1: kernels add their algorithmic bytes to kbytes (profiling)
   // Batched BFS: OR of the frontier masks of level parity p (the sources that
   // can still reach new vertices); accumulated while the level's masks are
   // produced, cleared once consumed.
@@ -76,15 +77,18 @@ enum KernelId : int {
   KID_OTHER = 11
 };
 
-// Adds a CTA's byte count to the run's counter for kernel kind `kid`
-// (one atomic per CTA; call from every thread with its own count).
-MG_DEVINL void add_bytes(unsigned long long *kbytes, int kid, unsigned long long mine) {
+// Adds a warp's byte count to the run's counter for kernel kind `kid` (one
+// atomic per warp; call from every thread with its own count). Only while
+// profiling: otherwise the counters are not read and the atomics, all on one
+// cache line, would be contended work at the end of every launch.
+MG_DEVINL void add_bytes(Ctl *ctl, int kid, unsigned long long mine) {
+  if (!ctl->count_bytes) return;
   mine += __shfl_xor_sync(0xffffffffu, mine, 16);
   mine += __shfl_xor_sync(0xffffffffu, mine, 8);
   mine += __shfl_xor_sync(0xffffffffu, mine, 4);
   mine += __shfl_xor_sync(0xffffffffu, mine, 2);
   mine += __shfl_xor_sync(0xffffffffu, mine, 1);
-  if ((threadIdx.x & 31) == 0 && mine) atomicAdd(&kbytes[kid], mine);
+  if ((threadIdx.x & 31) == 0 && mine) atomicAdd(&ctl->kbytes[kid], mine);
 }
 
 MG_DEVINL uint32_t ld_acquire(const uint32_t *p) {

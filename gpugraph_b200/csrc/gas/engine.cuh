@@ -37,6 +37,7 @@
 
 #include "../common.cuh"
 #include "../graph.cuh"
+#include "driver.cuh"
 #include "enums.h"
 
 namespace mg {
@@ -243,7 +244,7 @@ __global__ void __launch_bounds__(kNT) k_frontier_scan(GasArgs<P> a) {
       }
     }
   }
-  add_bytes(ctl->kbytes, KID_SCAN, my_bytes);
+  add_bytes(ctl, KID_SCAN, my_bytes);
 }
 
 // ------------------------------------------------------------ tile decode --
@@ -465,7 +466,7 @@ __global__ void __launch_bounds__(kNT) k_expand(GasArgs<P> a) {
                           Fout, (uint32_t)V, ctl))
       break;
   }
-  add_bytes(ctl->kbytes, KID_EXPAND, my_bytes);
+  add_bytes(ctl, KID_EXPAND, my_bytes);
   if (track_next_edges_trait<P>::value) {
     my_edges = warp_sum(my_edges);
     if (lane == 0 && my_edges) atomicAdd(&s_edges, my_edges);
@@ -508,7 +509,8 @@ static __global__ void k_sequence_i32(int32_t *p, int64_t n) {
     p[i] = (int32_t)i;
 }
 
-// flags: bit 0 = ordered frontier compaction (mg_options.ordered_frontier)
+// flags: bit 0 = ordered frontier compaction (mg_options.ordered_frontier),
+// bit 1 = count algorithmic bytes (profiling)
 MG_DEVINL void ctl_init_body(Ctl *ctl, uint32_t frontier_size, uint32_t max_iter, unsigned long long spin_limit,
                              uint32_t mode, uint32_t flags) {
   // The epoch keeps growing across runs so stale look-back words never match;
@@ -525,6 +527,7 @@ MG_DEVINL void ctl_init_body(Ctl *ctl, uint32_t frontier_size, uint32_t max_iter
   c.next_mode = mode;
   c.active = (frontier_size > 0 && max_iter > 0) ? 1u : 0u;
   c.ordered = flags & 1u;
+  c.count_bytes = (flags >> 1) & 1u;
   *ctl = c;
 }
 
@@ -533,6 +536,8 @@ static __global__ void k_ctl_init(Ctl *ctl, uint32_t frontier_size, uint32_t max
   if (threadIdx.x == 0) ctl_init_body(ctl, frontier_size, max_iter, spin_limit, mode, flags);
 }
 
-inline uint32_t ctl_flags(const mg_options *o) { return (o && o->ordered_frontier) ? 1u : 0u; }
+inline uint32_t ctl_flags(const mg_options *o) {
+  return ((o && o->ordered_frontier) ? 1u : 0u) | (prof_on() ? 2u : 0u);
+}
 
 }  // namespace mg

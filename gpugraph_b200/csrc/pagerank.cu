@@ -223,7 +223,7 @@ __global__ void __launch_bounds__(kNT, 6) k_pr_iter(PrArgs a) {
       my_bytes += 4 + 8ull * (unsigned long long)(ce - cb);
     }
   }
-  add_bytes(ctl->kbytes, KID_PR_PULL, my_bytes);
+  add_bytes(ctl, KID_PR_PULL, my_bytes);
   pr_flush(ctl, rs, rc, ds, dc);
 }
 
@@ -245,7 +245,7 @@ __global__ void __launch_bounds__(kNT) k_pr_fixup(PrArgs a) {
     pr_finalize(a, v, s, base, rold, rnew, cnew, rs, rc, ds, dc);
     my_bytes += 28 + 4ull * (unsigned long long)(a.heavy_first[h + 1] - a.heavy_first[h]);
   }
-  add_bytes(ctl->kbytes, KID_PR_PULL, my_bytes);
+  add_bytes(ctl, KID_PR_PULL, my_bytes);
   pr_flush(ctl, rs, rc, ds, dc);
 }
 
@@ -444,7 +444,7 @@ extern "C" int mg_pagerank(mg_graph *g, float *ranks, mg_stats *stats, const mg_
   a.damping = (float)d;
   a.ctl = g->ws.ctl;
   k_pr_init<<<g->num_sms * 4, 256, 0, s>>>(a.inv, a.r0, a.c0, V, (float)inv_n);
-  k_ctl_init<<<1, 32, 0, s>>>(a.ctl, 1u, max_iter, (unsigned long long)o->spin_limit, MODE_QUEUE, 0u);
+  k_ctl_init<<<1, 32, 0, s>>>(a.ctl, 1u, max_iter, (unsigned long long)o->spin_limit, MODE_QUEUE, ctl_flags(nullptr));
   count_launch(2);
   const double base0 = (1.0 - d) * inv_n + d * ((double)g->pr_ndangling * inv_n) * inv_n;
   cudaError_t e = cudaMemcpyAsync(&a.ctl->dangling, &base0, sizeof(double), cudaMemcpyHostToDevice, s);

@@ -114,7 +114,7 @@ __global__ void __launch_bounds__(kNT) k_ppr_iter(PprArgs a) {
       }
     }
   }
-  add_bytes(ctl->kbytes, KID_PPR, my_bytes);
+  add_bytes(ctl, KID_PPR, my_bytes);
   res = warp_sum(res);
   if (lane == 0 && res != 0.0) atomicAdd(&ctl->acc[1], res);
 }
@@ -166,7 +166,7 @@ __global__ void k_ppr_level_end(Ctl *ctl, double tol, cudaGraphConditionalHandle
 template <int NC>
 __global__ void __launch_bounds__(kNT) k_ppr_edge_grad(const int32_t *ro, const int32_t *col, int32_t V, int32_t nvec,
                                                        const float *lam, const float *R, float d, float *grad_w,
-                                                       unsigned long long *kbytes) {
+                                                       Ctl *ctl) {
   const int lane = lane_id();
   const uint32_t nwarps = gridDim.x * kNW;
   unsigned long long my_bytes = 0;
@@ -206,7 +206,7 @@ __global__ void __launch_bounds__(kNT) k_ppr_edge_grad(const int32_t *ro, const 
     }
     if (lane == 0) my_bytes += 4ull * nvec + (unsigned long long)(e - b) * (8ull + 4ull * nvec);
   }
-  add_bytes(kbytes, KID_PPR, my_bytes);
+  add_bytes(ctl, KID_PPR, my_bytes);
 }
 
 // L1 norm of the right-hand side into ctl->acc[2] (FP64 accumulation).
@@ -358,7 +358,7 @@ static int ppr_solve(mg_graph *g, int dir, const float *w, const float *rhs, flo
   // start from the right-hand side
   k_copy_f32<<<g->num_sms * 4, 256, 0, s>>>(rhs, a.x0, n);
   const uint32_t max_iter = (uint32_t)std::max<int32_t>(0, std::min<int32_t>(o->iter_num, 100000));
-  k_ctl_init<<<1, 32, 0, s>>>(a.ctl, 1u, max_iter, (unsigned long long)o->spin_limit, MODE_QUEUE, 0u);
+  k_ctl_init<<<1, 32, 0, s>>>(a.ctl, 1u, max_iter, (unsigned long long)o->spin_limit, MODE_QUEUE, ctl_flags(nullptr));
   k_ppr_rhs_norm<<<g->num_sms * 4, 256, 0, s>>>(rhs, n, a.ctl);
   count_launch(3);
   const int grid = persistent_grid(g, o, 4);
@@ -460,10 +460,10 @@ int mg_ppr_backward(mg_graph *g, const float *edge_weights, const float *ranks, 
   if (grad_edge_weights) {
     if (nvec > 32)
       k_ppr_edge_grad<2><<<grid, kNT, 0, s>>>(g->csr.row_offsets, g->csr.col, g->csr.V, nvec, lam, ranks,
-                                              (float)o->damping, grad_edge_weights, g->ws.ctl->kbytes);
+                                              (float)o->damping, grad_edge_weights, g->ws.ctl);
     else
       k_ppr_edge_grad<1><<<grid, kNT, 0, s>>>(g->csr.row_offsets, g->csr.col, g->csr.V, nvec, lam, ranks,
-                                              (float)o->damping, grad_edge_weights, g->ws.ctl->kbytes);
+                                              (float)o->damping, grad_edge_weights, g->ws.ctl);
     count_launch();
   }
   if (grad_teleport) {

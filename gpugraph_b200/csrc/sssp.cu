@@ -136,7 +136,7 @@ __global__ void __launch_bounds__(kNT, 5) k_sssp_relax(GasArgs<sssp_relax> a) {
                           Fout, (uint32_t)V, ctl))
       break;
   }
-  add_bytes(ctl->kbytes, KID_EXPAND, my_bytes);
+  add_bytes(ctl, KID_EXPAND, my_bytes);
 }
 
 __global__ void k_sssp_seed(int32_t *dist, int32_t *queue0, int32_t src) {
