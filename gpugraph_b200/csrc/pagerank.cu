@@ -73,12 +73,12 @@ MG_DEVINL void pr_finalize(const PrArgs &a, int v, float s, float base, const fl
   pr_store(a.damping, v, s, base, rold[v], a.inv[v], rnew, cnew, rs, rc, ds, dc);
 }
 
-// Reduces the per-thread compensated accumulators in FP64 into ctl->acc[1..2].
+// Reduces the per-thread compensated accumulators in FP64 into ctl->acc[1..2]
+// (one atomic per CTA and slot); called by every thread of the CTA.
 MG_DEVINL void pr_flush(Ctl *ctl, float rs, float rc, float ds, float dc) {
-  double r = (double)rs - (double)rc, d = (double)ds - (double)dc;
-  r = warp_sum(r);
-  d = warp_sum(d);
-  if (lane_id() == 0) {
+  const double r = cta_sum_f64((double)rs - (double)rc);
+  const double d = cta_sum_f64((double)ds - (double)dc);
+  if (threadIdx.x == 0) {
     if (r != 0.0) atomicAdd(&ctl->acc[1], r);
     if (d != 0.0) atomicAdd(&ctl->acc[2], d);
   }

@@ -115,8 +115,8 @@ __global__ void __launch_bounds__(kNT) k_ppr_iter(PprArgs a) {
     }
   }
   add_bytes(ctl, KID_PPR, my_bytes);
-  res = warp_sum(res);
-  if (lane == 0 && res != 0.0) atomicAdd(&ctl->acc[1], res);
+  res = cta_sum_f64(res);
+  if (threadIdx.x == 0 && res != 0.0) atomicAdd(&ctl->acc[1], res);
 }
 
 // Split vertices: partial rows added in chunk order.
@@ -143,8 +143,8 @@ __global__ void __launch_bounds__(kNT) k_ppr_fixup(PprArgs a) {
       }
     ppr_finalize_row<NC>(a, v, acc, xold, xnew, res);
   }
-  res = warp_sum(res);
-  if (lane == 0 && res != 0.0) atomicAdd(&ctl->acc[1], res);
+  res = cta_sum_f64(res);
+  if (threadIdx.x == 0 && res != 0.0) atomicAdd(&ctl->acc[1], res);
 }
 
 // ctl->acc[2] holds the L1 norm of the right-hand side (k_ppr_rhs_norm).
@@ -214,8 +214,8 @@ __global__ void k_ppr_rhs_norm(const float *rhs, int64_t n, Ctl *ctl) {
   double sum = 0.0;
   for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
     sum += fabs((double)rhs[i]);
-  sum = warp_sum(sum);
-  if (lane_id() == 0 && sum != 0.0) atomicAdd(&ctl->acc[2], sum);
+  sum = cta_sum_f64(sum);
+  if (threadIdx.x == 0 && sum != 0.0) atomicAdd(&ctl->acc[2], sum);
 }
 
 __global__ void k_scale_copy(const float *src, float *dst, float s, int64_t n) {
