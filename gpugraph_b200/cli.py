@@ -5,6 +5,7 @@
     python -m gpugraph_b200.cli bfs -g graph.mtx -s srcs.txt -o out.txt
     python -m gpugraph_b200.cli sssp --rmat 20 -p "src=0 direction=push"
     python -m gpugraph_b200.cli bfs_multi --rmat 22 --nsrc 64 --repeat 3
+    python -m gpugraph_b200.cli ppr --rmat 20 --directed --nsrc 32
 
 Parameters (-p / -c) use the reference's knob names where they exist:
 src, directed, iter_num, threshold, tol (PageRank), plus direction
@@ -57,9 +58,44 @@ def options_from(params: dict) -> dict:
     return kw
 
 
+def run_ppr(g: Graph, hg: HostGraph, nvec: int, seed: int, tol: float):
+    """Differentiable personalised PageRank, forward and backward of the loss
+    <C, R>: lognormal(0, 1) edge weights normalised per row, nvec teleport
+    vectors each uniform over 100 seeded vertices, C ~ N(0, 1). Returns the
+    ranks [V, nvec] and device time / iteration counts of both passes."""
+    import torch
+
+    from .ppr import ppr
+
+    rng = np.random.default_rng(seed)
+    w = rng.lognormal(0.0, 1.0, size=hg.edges)
+    src = np.repeat(np.arange(hg.nodes), np.diff(hg.row_offsets))
+    w = w / np.bincount(src, weights=w, minlength=hg.nodes)[src]
+    k = min(100, hg.nodes)
+    tele = np.zeros((hg.nodes, nvec), np.float32)
+    for c in range(nvec):
+        tele[rng.choice(hg.nodes, k, replace=False), c] = 1.0 / k
+    wt = torch.tensor(w, dtype=torch.float32, device="cuda", requires_grad=True)
+    tt = torch.tensor(tele, device="cuda", requires_grad=True)
+    cm = torch.tensor(rng.standard_normal((hg.nodes, nvec)), dtype=torch.float32, device="cuda")
+    e0, e1, e2 = (torch.cuda.Event(enable_timing=True) for _ in range(3))
+    e0.record()
+    r = ppr(g, wt, tt, tol=tol)
+    e1.record()
+    (r * cm).sum().backward()
+    e2.record()
+    torch.cuda.synchronize()
+    fwd, total = e0.elapsed_time(e1), e0.elapsed_time(e2)
+    print(f"ppr: {nvec} vectors, forward {fwd:.3f} ms, backward {total - fwd:.3f} ms", file=sys.stderr)
+    st = {"device_ms": total, "iterations": 0, "push_iterations": 0, "pull_iterations": 0,
+          "edges_traversed": 0}
+    return r.detach().cpu().numpy(), st
+
+
 def main(argv=None) -> int:
     ap = argparse.ArgumentParser(prog="gpugraph_b200.cli")
-    ap.add_argument("algo", choices=["bfs", "bfs_multi", "sssp", "sssp_multi", "cc", "pagerank", "pagerank_gas"])
+    ap.add_argument("algo", choices=["bfs", "bfs_multi", "sssp", "sssp_multi", "cc", "pagerank", "pagerank_gas",
+                                     "ppr"])
     ap.add_argument("-g", "--graph")
     ap.add_argument("-o", "--output")
     ap.add_argument("-s", "--sources")
@@ -124,6 +160,8 @@ def main(argv=None) -> int:
             result, st = g.cc(**kw)
         elif args.algo == "pagerank":
             result, st = g.pagerank(**({"tolerance": float(params["tol"])} if "tol" in params else {}), **kw)
+        elif args.algo == "ppr":
+            result, st = run_ppr(g, hg, args.nsrc, args.seed, float(params.get("tol", 1e-7)))
         else:
             result, st = g.pagerank_gas(tolerance=float(params.get("tol", 0.01)), **kw)
         wall = (time.perf_counter() - t0) * 1e3

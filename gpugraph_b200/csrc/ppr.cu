@@ -161,48 +161,55 @@ __global__ void k_ppr_level_end(Ctl *ctl, double tol, cudaGraphConditionalHandle
   if (use_handle) cudaGraphSetConditional(h, ctl->active);
 }
 
-// dL/dw(u,v) = d <lambda[v,:], R[u,:]>: warp per row u, R[u,:] held in registers,
-// four out-edges reduced per step.
+// dL/dw(u,v) = d <lambda[v,:], R[u,:]>: warp per out-edge chunk of the CSR
+// chunk plan (a row, or at most kPprChunk edges of a long row, so a hub's row
+// is spread over many warps), R[u,:] held in registers, EPS out-edges per step
+// with all their row gathers in flight before the warp reductions.
 template <int NC>
-__global__ void __launch_bounds__(kNT) k_ppr_edge_grad(const int32_t *ro, const int32_t *col, int32_t V, int32_t nvec,
+__global__ void __launch_bounds__(kNT) k_ppr_edge_grad(const int32_t *cv, const int32_t *cb, const int32_t *ce,
+                                                       int32_t nchunks, const int32_t *col, int32_t nvec,
                                                        const float *lam, const float *R, float d, float *grad_w,
                                                        Ctl *ctl) {
+  constexpr int EPS = NC == 1 ? 8 : 4;
   const int lane = lane_id();
   const uint32_t nwarps = gridDim.x * kNW;
   unsigned long long my_bytes = 0;
-  for (uint32_t u = blockIdx.x * kNW + warp_id(); u < (uint32_t)V; u += nwarps) {
-    const int b = ro[u], e = ro[u + 1];
+  for (uint32_t c = blockIdx.x * kNW + warp_id(); c < (uint32_t)nchunks; c += nwarps) {
+    const int u = cv[c], b = cb[c], e = ce[c];
     if (b == e) continue;
     float ru[NC];
 #pragma unroll
     for (int q = 0; q < NC; ++q) {
-      const int c = lane + 32 * q;
-      ru[q] = (c < nvec) ? R[(int64_t)u * nvec + c] : 0.f;
+      const int cc = lane + 32 * q;
+      ru[q] = (cc < nvec) ? R[(int64_t)u * nvec + cc] : 0.f;
     }
-    for (int k = b; k < e; k += 4) {
-      float dot[4];
+    for (int k = b; k < e; k += EPS) {
+      int v[EPS];
 #pragma unroll
-      for (int j = 0; j < 4; ++j) {
+      for (int j = 0; j < EPS; ++j) v[j] = (k + j < e) ? col[k + j] : -1;
+      float dot[EPS];
+#pragma unroll
+      for (int j = 0; j < EPS; ++j) {
         dot[j] = 0.f;
-        if (k + j < e) {
-          const int v = col[k + j];
+        if (v[j] >= 0) {
 #pragma unroll
           for (int q = 0; q < NC; ++q) {
-            const int c = lane + 32 * q;
-            if (c < nvec) dot[j] = fmaf(__ldg(&lam[(int64_t)v * nvec + c]), ru[q], dot[j]);
+            const int cc = lane + 32 * q;
+            if (cc < nvec) dot[j] = fmaf(__ldg(&lam[(int64_t)v[j] * nvec + cc]), ru[q], dot[j]);
           }
         }
       }
 #pragma unroll
-      for (int j = 0; j < 4; ++j) {
+      for (int j = 0; j < EPS; ++j) {
 #pragma unroll
         for (int o = 16; o > 0; o >>= 1) dot[j] += __shfl_xor_sync(0xffffffffu, dot[j], o);
       }
-      if (lane == 0) {
+      // lane j writes edge k + j
+      float mine = dot[0];
 #pragma unroll
-        for (int j = 0; j < 4; ++j)
-          if (k + j < e) grad_w[k + j] = d * dot[j];
-      }
+      for (int j = 1; j < EPS; ++j)
+        if (lane == j) mine = dot[j];
+      if (lane < EPS && k + lane < e) grad_w[k + lane] = d * mine;
     }
     if (lane == 0) my_bytes += 4ull * nvec + (unsigned long long)(e - b) * (8ull + 4ull * nvec);
   }
@@ -458,11 +465,12 @@ int mg_ppr_backward(mg_graph *g, const float *edge_weights, const float *ranks, 
   if ((st = ppr_solve(g, 1, edge_weights, grad_ranks, 1.0f, nvec, o, s, "ppr_adj", &lam, &res)) != MG_OK) return st;
   const int grid = persistent_grid(g, o, 4);
   if (grad_edge_weights) {
+    const mg_graph::PprPlan &pl = g->ppr_plan[1];  // chunks of the out-edge rows
     if (nvec > 32)
-      k_ppr_edge_grad<2><<<grid, kNT, 0, s>>>(g->csr.row_offsets, g->csr.col, g->csr.V, nvec, lam, ranks,
+      k_ppr_edge_grad<2><<<grid, kNT, 0, s>>>(pl.cv, pl.cb, pl.ce, pl.nchunks, g->csr.col, nvec, lam, ranks,
                                               (float)o->damping, grad_edge_weights, g->ws.ctl);
     else
-      k_ppr_edge_grad<1><<<grid, kNT, 0, s>>>(g->csr.row_offsets, g->csr.col, g->csr.V, nvec, lam, ranks,
+      k_ppr_edge_grad<1><<<grid, kNT, 0, s>>>(pl.cv, pl.cb, pl.ce, pl.nchunks, g->csr.col, nvec, lam, ranks,
                                               (float)o->damping, grad_edge_weights, g->ws.ctl);
     count_launch();
   }
