@@ -119,6 +119,78 @@ __global__ void __launch_bounds__(kNT) k_ppr_iter(PprArgs a) {
   if (threadIdx.x == 0 && res != 0.0) atomicAdd(&ctl->acc[1], res);
 }
 
+// Vector variant for nvec % 4 == 0 (rows 16-byte aligned): a group of G lanes
+// owns one chunk and lane l of the group columns 4l..4l+3, one 16-byte load
+// per gathered row, so a warp works on 32/G chunks at once (4 for nvec <= 32,
+// 2 for nvec <= 64): that many chunks' index, weight and row loads are in
+// flight per step instead of one. Per column the edges are added in the same
+// order as in k_ppr_iter, so both give the same ranks.
+template <int G>
+__global__ void __launch_bounds__(kNT, 4) k_ppr_iter_v(PprArgs a) {
+  constexpr int PER = 32 / G;
+  constexpr int EPS = 8;
+  Ctl *ctl = a.ctl;
+  if (!ctl->active) return;
+  const uint32_t L = ctl->level;
+  const float *xold = (L & 1) ? a.x1 : a.x0;
+  float *xnew = (L & 1) ? a.x0 : a.x1;
+  const int lane = lane_id();
+  const int gl = lane & (G - 1);
+  const int col = gl * 4;
+  const bool cok = col < a.nvec;
+  double res = 0.0;
+  unsigned long long my_bytes = 0;
+  const uint32_t nslots = gridDim.x * kNW * PER;
+  for (uint32_t c = (blockIdx.x * kNW + warp_id()) * PER + lane / G; c < (uint32_t)a.nchunks; c += nslots) {
+    const int v = a.cv[c], b = a.cb[c], e = a.ce[c], slot = a.cslot[c];
+    float4 acc = make_float4(0.f, 0.f, 0.f, 0.f);
+    for (int k = b; k < e; k += EPS) {
+      int u[EPS];
+      float wt[EPS];
+#pragma unroll
+      for (int j = 0; j < EPS; ++j) {
+        const bool in = k + j < e;
+        u[j] = in ? a.idx[k + j] : -1;
+        wt[j] = in ? a.w[a.eid ? a.eid[k + j] : k + j] : 0.f;
+      }
+      float4 row[EPS];
+#pragma unroll
+      for (int j = 0; j < EPS; ++j)
+        row[j] = (u[j] >= 0 && cok) ? __ldg(reinterpret_cast<const float4 *>(xold + (int64_t)u[j] * a.nvec + col))
+                                    : make_float4(0.f, 0.f, 0.f, 0.f);
+#pragma unroll
+      for (int j = 0; j < EPS; ++j) {
+        acc.x = fmaf(wt[j], row[j].x, acc.x);
+        acc.y = fmaf(wt[j], row[j].y, acc.y);
+        acc.z = fmaf(wt[j], row[j].z, acc.z);
+        acc.w = fmaf(wt[j], row[j].w, acc.w);
+      }
+    }
+    if (gl == 0) my_bytes += (unsigned long long)(e - b) * (8ull + 4ull * a.nvec);
+    if (slot < 0) {
+      if (cok) {
+        const int64_t o = (int64_t)v * a.nvec + col;
+        const float4 r = *reinterpret_cast<const float4 *>(a.rhs + o);
+        const float4 xo = *reinterpret_cast<const float4 *>(xold + o);
+        float4 xn;
+        xn.x = fmaf(a.d, acc.x, a.alpha * r.x);
+        xn.y = fmaf(a.d, acc.y, a.alpha * r.y);
+        xn.z = fmaf(a.d, acc.z, a.alpha * r.z);
+        xn.w = fmaf(a.d, acc.w, a.alpha * r.w);
+        res += (double)fabsf(xn.x - xo.x) + (double)fabsf(xn.y - xo.y) + (double)fabsf(xn.z - xo.z) +
+               (double)fabsf(xn.w - xo.w);
+        *reinterpret_cast<float4 *>(xnew + o) = xn;
+      }
+      if (gl == 0) my_bytes += 12ull * a.nvec;
+    } else if (cok) {
+      *reinterpret_cast<float4 *>(a.partial + (int64_t)slot * a.nvec + col) = acc;
+    }
+  }
+  add_bytes(ctl, KID_PPR, my_bytes);
+  res = cta_sum_f64(res);
+  if (threadIdx.x == 0 && res != 0.0) atomicAdd(&ctl->acc[1], res);
+}
+
 // Split vertices: partial rows added in chunk order.
 template <int NC>
 __global__ void __launch_bounds__(kNT) k_ppr_fixup(PprArgs a) {
@@ -371,12 +443,15 @@ static int ppr_solve(mg_graph *g, int dir, const float *w, const float *rhs, flo
   const int grid = persistent_grid(g, o, 4);
   const double tol = o->tolerance;
   const bool two = nvec > 32;
+  const bool vec = nvec % 4 == 0;  // 16-byte rows: the vector variant
   LevelBody body = [=](cudaStream_t ss, cudaGraphConditionalHandle h, int use_h) {
     if (two) {
-      MG_LAUNCH(KID_PPR, ss, k_ppr_iter<2><<<grid, kNT, 0, ss>>>(a));
+      if (vec) MG_LAUNCH(KID_PPR, ss, k_ppr_iter_v<16><<<grid, kNT, 0, ss>>>(a));
+      else MG_LAUNCH(KID_PPR, ss, k_ppr_iter<2><<<grid, kNT, 0, ss>>>(a));
       MG_LAUNCH(KID_PPR, ss, k_ppr_fixup<2><<<grid, kNT, 0, ss>>>(a));
     } else {
-      MG_LAUNCH(KID_PPR, ss, k_ppr_iter<1><<<grid, kNT, 0, ss>>>(a));
+      if (vec) MG_LAUNCH(KID_PPR, ss, k_ppr_iter_v<8><<<grid, kNT, 0, ss>>>(a));
+      else MG_LAUNCH(KID_PPR, ss, k_ppr_iter<1><<<grid, kNT, 0, ss>>>(a));
       MG_LAUNCH(KID_PPR, ss, k_ppr_fixup<1><<<grid, kNT, 0, ss>>>(a));
     }
     MG_LAUNCH(KID_OTHER, ss, k_ppr_level_end<<<1, 32, 0, ss>>>(a.ctl, tol, h, use_h));

@@ -40,10 +40,13 @@ def _dense_solve(hg, src, w, T):
     return torch.linalg.solve(A, (1 - D) * T), P
 
 
-def test_ppr_forward_matches_dense_fp64():
+@pytest.mark.parametrize("nvec", [32, 5, 12, 40, 64])
+def test_ppr_forward_matches_dense_fp64(nvec):
+    # nvec % 4 == 0 runs the 16-byte-row kernel (4 or 2 chunks per warp), other
+    # counts the column-per-lane kernel; nvec > 32 takes two columns per lane
     from gpugraph_b200.ppr import ppr
 
-    hg, g, src, w, T, _ = _setup()
+    hg, g, src, w, T, _ = _setup(nvec=nvec)
     R_ref, _ = _dense_solve(hg, src, w, torch.as_tensor(T))
     R = ppr(g, torch.tensor(w, dtype=torch.float32, device="cuda"), torch.tensor(T, dtype=torch.float32,
                                                                                device="cuda"))
@@ -98,6 +101,28 @@ def test_ppr_gradients_vs_dense_autograd_and_finite_differences():
         Tm[v, c] -= h
         fd = (L_of(base_w, Tp) - L_of(base_w, Tm)) / (2 * h)
         assert abs(fd - float(gT[v, c])) <= 1e-3 * max(1.0, abs(fd)), (v, c, fd, float(gT[v, c]))
+
+
+@pytest.mark.parametrize("nvec", [40, 7])
+def test_ppr_gradients_other_column_counts(nvec):
+    # two columns per lane (nvec > 32, 16-byte rows) and the column-per-lane
+    # kernel (nvec = 7) against the dense FP64 autograd gradient
+    from gpugraph_b200.ppr import ppr
+
+    hg, g, src, w, T, Cm = _setup(nvec=nvec, seed=2)
+    wt = torch.tensor(w, dtype=torch.float32, device="cuda", requires_grad=True)
+    Tt = torch.tensor(T, dtype=torch.float32, device="cuda", requires_grad=True)
+    (ppr(g, wt, Tt) * torch.tensor(Cm, dtype=torch.float32, device="cuda")).sum().backward()
+    w64 = torch.tensor(w, dtype=torch.float64, requires_grad=True)
+    T64 = torch.tensor(T, dtype=torch.float64, requires_grad=True)
+    n = hg.nodes
+    P = torch.zeros((n, n), dtype=torch.float64).index_put(
+        (torch.as_tensor(src), torch.as_tensor(hg.column_indices.astype(np.int64))), w64, accumulate=True)
+    R64 = torch.linalg.solve(torch.eye(n, dtype=torch.float64) - D * P.T, (1 - D) * T64)
+    (R64 * torch.tensor(Cm)).sum().backward()
+    rel_w = (wt.grad.double().cpu() - w64.grad).norm() / w64.grad.norm()
+    rel_t = (Tt.grad.double().cpu() - T64.grad).norm() / T64.grad.norm()
+    assert rel_w < 1e-4 and rel_t < 1e-4, (float(rel_w), float(rel_t))
 
 
 def test_ppr_rejects_symmetric_graph_and_host_pointers():
