@@ -58,7 +58,7 @@ def options_from(params: dict) -> dict:
     return kw
 
 
-def run_ppr(g: Graph, hg: HostGraph, nvec: int, seed: int, tol: float):
+def run_ppr(g: Graph, hg: HostGraph, nvec: int, seed: int, tol: float, options: dict | None = None):
     """Differentiable personalised PageRank, forward and backward of the loss
     <C, R>: lognormal(0, 1) edge weights normalised per row, nvec teleport
     vectors each uniform over 100 seeded vertices, C ~ N(0, 1). Returns the
@@ -80,7 +80,7 @@ def run_ppr(g: Graph, hg: HostGraph, nvec: int, seed: int, tol: float):
     cm = torch.tensor(rng.standard_normal((hg.nodes, nvec)), dtype=torch.float32, device="cuda")
     e0, e1, e2 = (torch.cuda.Event(enable_timing=True) for _ in range(3))
     e0.record()
-    r = ppr(g, wt, tt, tol=tol)
+    r = ppr(g, wt, tt, tol=tol, **{k: v for k, v in (options or {}).items() if k == "use_cuda_graph"})
     e1.record()
     (r * cm).sum().backward()
     e2.record()
@@ -161,7 +161,7 @@ def main(argv=None) -> int:
         elif args.algo == "pagerank":
             result, st = g.pagerank(**({"tolerance": float(params["tol"])} if "tol" in params else {}), **kw)
         elif args.algo == "ppr":
-            result, st = run_ppr(g, hg, args.nsrc, args.seed, float(params.get("tol", 1e-7)))
+            result, st = run_ppr(g, hg, args.nsrc, args.seed, float(params.get("tol", 1e-7)), kw)
         else:
             result, st = g.pagerank_gas(tolerance=float(params.get("tol", 0.01)), **kw)
         wall = (time.perf_counter() - t0) * 1e3

@@ -207,7 +207,25 @@ __global__ void __launch_bounds__(kNT) k_ppr_fixup(PprArgs a) {
     float acc[NC];
 #pragma unroll
     for (int q = 0; q < NC; ++q) acc[q] = 0.f;
-    for (int s = a.mfirst[m]; s < a.mfirst[m + 1]; ++s)
+    // eight partial rows loaded at once, then added in chunk order (a hub has
+    // hundreds of chunks; one dependent load per chunk made this the tail)
+    int s = a.mfirst[m];
+    const int se = a.mfirst[m + 1];
+    for (; s + 8 <= se; s += 8) {
+      float t[8][NC];
+#pragma unroll
+      for (int j = 0; j < 8; ++j)
+#pragma unroll
+        for (int q = 0; q < NC; ++q) {
+          const int col = lane + 32 * q;
+          t[j][q] = col < a.nvec ? a.partial[(int64_t)(s + j) * a.nvec + col] : 0.f;
+        }
+#pragma unroll
+      for (int j = 0; j < 8; ++j)
+#pragma unroll
+        for (int q = 0; q < NC; ++q) acc[q] += t[j][q];
+    }
+    for (; s < se; ++s)
 #pragma unroll
       for (int q = 0; q < NC; ++q) {
         const int col = lane + 32 * q;

@@ -23,7 +23,7 @@ from ._lib import check, default_options, lib
 
 class _PPR(torch.autograd.Function):
     @staticmethod
-    def forward(ctx, edge_weights, teleport, graph, damping, tol, max_iter):
+    def forward(ctx, edge_weights, teleport, graph, damping, tol, max_iter, extra):
         w = edge_weights.detach().contiguous()
         t = teleport.detach().contiguous()
         if w.dtype != torch.float32 or t.dtype != torch.float32 or not w.is_cuda or not t.is_cuda:
@@ -33,11 +33,11 @@ class _PPR(torch.autograd.Function):
         nvec = int(t.shape[1])
         out = torch.empty_like(t)
         o = default_options(damping=damping, tolerance=tol, iter_num=max_iter,
-                            stream=torch.cuda.current_stream().cuda_stream)
+                            stream=torch.cuda.current_stream().cuda_stream, **extra)
         st = _lib.Stats()
         check(lib.mg_ppr_forward(graph.handle, w.data_ptr(), t.data_ptr(), nvec, out.data_ptr(), C.byref(st),
                                  C.byref(o)), "mg_ppr_forward")
-        ctx.graph, ctx.damping, ctx.tol, ctx.max_iter = graph, damping, tol, max_iter
+        ctx.graph, ctx.damping, ctx.tol, ctx.max_iter, ctx.extra = graph, damping, tol, max_iter, extra
         ctx.forward_stats = st.as_dict()
         ctx.save_for_backward(w, out)
         return out
@@ -51,16 +51,17 @@ class _PPR(torch.autograd.Function):
         gw = torch.empty_like(w) if need_w else None
         gt = torch.empty_like(R) if need_t else None
         o = default_options(damping=ctx.damping, tolerance=ctx.tol, iter_num=ctx.max_iter,
-                            stream=torch.cuda.current_stream().cuda_stream)
+                            stream=torch.cuda.current_stream().cuda_stream, **ctx.extra)
         st = _lib.Stats()
         check(lib.mg_ppr_backward(ctx.graph.handle, w.data_ptr(), R.data_ptr(), g.data_ptr(), nvec,
                                   gw.data_ptr() if gw is not None else None,
                                   gt.data_ptr() if gt is not None else None, C.byref(st), C.byref(o)),
               "mg_ppr_backward")
-        return gw, gt, None, None, None, None
+        return gw, gt, None, None, None, None, None
 
 
 def ppr(graph, edge_weights: torch.Tensor, teleport: torch.Tensor, damping: float = 0.85, tol: float = 1e-7,
-        max_iter: int = 10000) -> torch.Tensor:
-    """Personalised PageRank of every teleport column; differentiable in both inputs."""
-    return _PPR.apply(edge_weights, teleport, graph, damping, tol, max_iter)
+        max_iter: int = 10000, **options) -> torch.Tensor:
+    """Personalised PageRank of every teleport column; differentiable in both inputs.
+    `options`: further mg_options fields for both passes (e.g. use_cuda_graph=0)."""
+    return _PPR.apply(edge_weights, teleport, graph, damping, tol, max_iter, dict(options))
