@@ -183,6 +183,7 @@ def run_native(args, rank: int, world: int):
     o_stats = _lib.default_options(**dict(base_opts, compute_stats=1))
     _lib.check(lib.mg_bfs_multi(g.handle, src_arr.ctypes.data, NSRC, out_dev.data_ptr(), st, o_stats), "stats")
     teps_edges = int(st.edges_traversed)
+    reached_total = int(st.vertices_reached)
     levels_multi = (st.iterations, st.push_iterations, st.pull_iterations)
 
     for _ in range(args.warmup):
@@ -230,10 +231,18 @@ def run_native(args, rank: int, world: int):
         _lib.check(lib.mg_bfs(g.handle, int(srcs[k]), one.data_ptr(), None, o_single), "mg_bfs")
         parity &= bool(torch.equal(one, out_dev[k]))
 
+    # path-level bytes of the 64 single-source BFS (8 B per traversed edge + 20 B per reached vertex),
+    # over the API-timed run and over the level loops alone, against the measured copy bandwidth
+    path_bytes = 8 * teps_edges + 20 * reached_total
+    peak = measured_peak_hbm()[0]
     sub = {"bfs_batched64": {"gteps": value / world, "ms": ms_step, "levels": levels_multi},
            "bfs_single_x64": {"gteps": single_gteps, "ms_total": single_ms, "ms_per_source": single_ms / NSRC,
                               "device_ms_sum": dev_sum,
-                              "gteps_device_only": teps_edges / (dev_sum * 1e-3) / 1e9 if dev_sum else None},
+                              "gteps_device_only": teps_edges / (dev_sum * 1e-3) / 1e9 if dev_sum else None,
+                              "path_bytes": path_bytes,
+                              "path_hbm_frac": path_bytes / (single_ms * 1e-3) / 1e9 / peak,
+                              "path_hbm_frac_level_loops": (path_bytes / (dev_sum * 1e-3) / 1e9 / peak
+                                                            if dev_sum else None)},
            "batched_over_single": value / world / single_gteps,
            "batched_over_single_device_only": (dev_sum / ms_step) if dev_sum else None,
            "batched_equals_single_spot_check": parity}
