@@ -553,6 +553,7 @@ __global__ void __launch_bounds__(kNT) k_mss_expand(MultiArgs a, const uint32_t 
   __shared__ int32_t s_base[NV + 1];
   __shared__ int32_t s_rs[NV + 1];
   __shared__ int32_t s_own[NV];
+  __shared__ int32_t s_q[NV];  // per warp: its queued vertices of the current tile
   __shared__ uint32_t s_tile;
   __shared__ int s_fail;
   Ctl *ctl = a.ctl;
@@ -608,7 +609,13 @@ __global__ void __launch_bounds__(kNT) k_mss_expand(MultiArgs a, const uint32_t 
       w = wgt[eid];
       am = Fc[u];
     };
-    // next-level mask, dedup bit and queue slot for the vertices that improved
+    // next-level mask and dedup bit of the vertices that improved; the ones
+    // that won the dedup bit are staged in the warp's part of s_q (an item
+    // queues at most one vertex, so PER_WARP slots suffice) and reserved in the
+    // queue once per warp and tile (a reservation per step was a same-address
+    // atomic for every 32 or 4 edges)
+    int32_t *wq = s_q + warp * PER_WARP;
+    int qn = 0;  // warp-uniform
     auto enqueue = [&](bool has, int v, u64 mask) {
       bool enq = false;
       if (has) {
@@ -617,18 +624,13 @@ __global__ void __launch_bounds__(kNT) k_mss_expand(MultiArgs a, const uint32_t 
         const uint32_t bit = 1u << (v & 31);
         enq = !(ld_volatile(&dedup[v >> 5]) & bit) && !(atomicOr(&dedup[v >> 5], bit) & bit);
       }
-      // one queue reservation per warp step
       const uint32_t eb = __ballot_sync(0xffffffffu, enq);
-      if (eb) {
-        uint32_t base = 0;
-        if (lane == 0) base = atomicAdd(&ctl->next_size, (uint32_t)__popc(eb));
-        base = __shfl_sync(0xffffffffu, base, 0);
-        if (enq) {
-          const uint32_t pos = base + __popc(eb & lanemask_lt());
-          if (pos < (uint32_t)V) Qn[pos] = v;
-          else raise_error(ctl, MG_ERR_OVERFLOW);
-        }
+      if (enq) {
+        const int pos = qn + __popc(eb & lanemask_lt());
+        if (pos < PER_WARP) wq[pos] = v;
+        else raise_error(ctl, MG_ERR_OVERFLOW);
       }
+      qn = min(qn + __popc(eb), PER_WARP);
     };
     int nu = -1, nv = 0, nw = 0;
     u64 nam = 0;
@@ -681,6 +683,16 @@ __global__ void __launch_bounds__(kNT) k_mss_expand(MultiArgs a, const uint32_t 
         mask |= __shfl_xor_sync(0xffffffffu, mask, 2);
         mask |= __shfl_xor_sync(0xffffffffu, mask, 4);
         enqueue(sub == 0 && mask != 0, v, mask);
+      }
+    }
+    __syncwarp();
+    if (qn) {
+      uint32_t base = 0;
+      if (lane == 0) base = atomicAdd(&ctl->next_size, (uint32_t)qn);
+      base = __shfl_sync(0xffffffffu, base, 0);
+      for (int i = lane; i < qn; i += 32) {
+        if (base + (uint32_t)i < (uint32_t)V) Qn[base + i] = wq[i];
+        else raise_error(ctl, MG_ERR_OVERFLOW);
       }
     }
   }
