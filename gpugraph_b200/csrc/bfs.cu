@@ -5,8 +5,9 @@
 // and stops at the first hit.
 // The switch follows Beamer's rule: push -> pull when the next frontier's
 // out-edges exceed (unvisited edges)/alpha while the frontier grows, pull ->
-// push when the frontier shrinks below nodes/beta. Depths are unique, so every schedule gives the
-// same labels as the reference's CPUBFS (Algorithms/BFS/bfs.cu:57-111).
+// push when the frontier shrinks below nodes/beta. Depths are unique, so every
+// schedule gives the same labels as the reference's CPUBFS
+// (Algorithms/BFS/bfs.cu:57-111).
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -494,7 +495,7 @@ int bfs_run(mg_graph *g, const std::vector<int32_t> &roots, int32_t *depths, mg_
   // Every level of a traversal settles at least one vertex, so V + 2 levels bound
   // the device loop even if a Program never empties its frontier.
   const uint32_t max_iter = (uint32_t)std::min<int64_t>(o->iter_num > 0 ? o->iter_num : 0, g->nodes + 2);
-  // one root goes to the init kernel by value; several are copied
+  // one root goes to the start kernel by value; several are copied to the queue
   const int queue0_ready = nsrc > 1 ? 1 : 0;
   if (queue0_ready) {
     cudaError_t e = cudaMemcpyAsync(w.queue[0], roots.data(), nsrc * 4, cudaMemcpyHostToDevice, s);
