@@ -374,7 +374,6 @@ __global__ void k_bfs_level_end(Ctl *ctl, int32_t V, int64_t E, cudaGraphConditi
       if ((double)n_next < (double)V / (double)ctl->beta && n_next < ctl->frontier_size) new_mode = MODE_QUEUE;
     }
     ctl->convert = (mode == MODE_BITMAP && new_mode == MODE_QUEUE) ? 1u : 0u;
-    ctl->group_ctr = 0;
     ctl->mode = new_mode;
     ctl->level += 1;
     ctl->frontier_size = n_next;

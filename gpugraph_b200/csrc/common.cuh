@@ -40,7 +40,6 @@ struct Ctl {
   uint32_t dir_policy;      // MG_DIR_* (BFS)
   uint32_t convert;         // 1: rebuild the queue from the bitmap at level start
   uint32_t ordered;         // 1: compact the next frontier in tile order (look-back)
-  uint32_t group_ctr;       // dynamic work counter of the pull kernels
   uint32_t prev_size;       // |F| of the previous level (batched traversals)
   uint32_t apply_pending;   // 1: the previous push level left bits to apply
   uint32_t count_bytes;     // 1: kernels add their algorithmic bytes to kbytes (profiling)

@@ -429,7 +429,6 @@ __global__ void k_ms_level_end(Ctl *ctl, int32_t V, int64_t E, cudaGraphConditio
       if ((double)n_next < (double)V / (double)ctl->beta && n_next < ctl->frontier_size) new_mode = MODE_QUEUE;
     }
     ctl->srcmask[ctl->level & 1] = 0;  // consumed; the level after next accumulates it afresh
-    ctl->group_ctr = 0;
     ctl->apply_pending = (mode == MODE_QUEUE) ? 1u : 0u;
     ctl->convert = (mode == MODE_BITMAP && new_mode == MODE_QUEUE) ? 1u : 0u;
     ctl->mode = new_mode;
