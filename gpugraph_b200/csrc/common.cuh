@@ -237,21 +237,4 @@ MG_DEVINL uint32_t next_tile(uint32_t *ctr, uint32_t *smem_slot) {
   return *smem_slot;
 }
 
-// "Last CTA out" detection: returns true in exactly one CTA, after every other
-// CTA of the grid has passed this point (their prior writes are visible).
-MG_DEVINL bool last_cta_done(uint32_t *counter, uint32_t *smem_flag) {
-  __syncthreads();
-  if (threadIdx.x == 0) {
-    __threadfence();
-    uint32_t prev = atomicAdd(counter, 1u);
-    *smem_flag = (prev == gridDim.x - 1) ? 1u : 0u;
-    if (*smem_flag) {
-      __threadfence();
-      *counter = 0;  // ready for the next launch
-    }
-  }
-  __syncthreads();
-  return *smem_flag != 0;
-}
-
 }  // namespace mg
