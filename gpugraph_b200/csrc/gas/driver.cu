@@ -10,7 +10,7 @@
 namespace mg {
 
 constexpr size_t kMaxCachedLoops = 64;
-constexpr int kLevelsPerIteration = 2;
+constexpr int kLevelsPerIteration = 4;
 
 int read_ctl(mg_graph *g, cudaStream_t s, Ctl *out) {
   cudaError_t e = cudaMemcpyAsync(g->host_ctl, g->ws.ctl, sizeof(Ctl), cudaMemcpyDeviceToHost, s);
@@ -102,9 +102,9 @@ static int build_graph(mg_graph *g, cudaStream_t s, const LevelBody &body, LoopC
     cudaGraph_t bodyg = params.conditional.phGraph_out[0];
     e = cudaStreamBeginCaptureToGraph(s, bodyg, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal);
     if (e == cudaSuccess) {
-      // two levels per iteration of the WHILE node (a node iteration costs about
-      // as much as four empty kernels): when the first level ends the loop, the
-      // second copy's kernels return at once, as in the host-driven loop
+      // four levels per iteration of the WHILE node (a node iteration costs
+      // about as much as four empty kernels): when a level ends the loop, the
+      // later copies' kernels return at once, as in the host-driven loop
       for (int k = 0; k < kLevelsPerIteration; ++k) body(s, h, 1);
       cudaGraph_t captured = nullptr;
       cudaError_t e2 = cudaStreamEndCapture(s, &captured);
