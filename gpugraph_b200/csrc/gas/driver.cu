@@ -1,5 +1,6 @@
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <cstring>
 #include <vector>
 
@@ -184,7 +185,12 @@ int run_level_loop(mg_graph *g, cudaStream_t s, const std::string &key, int kern
   cudaEventElapsedTime(&ms, g->ev0, g->ev1);
   res->ms = ms;
   res->used_graph = graphed;
-  if (graphed) count_launch((int64_t)kernels_per_level * ((int64_t)res->ctl.level + 1));
+  if (graphed) {
+    // every iteration of the WHILE node launches all its level copies
+    const int64_t iters = std::max<int64_t>(1, ((int64_t)res->ctl.level + kLevelsPerIteration - 1) /
+                                                   kLevelsPerIteration);
+    count_launch((int64_t)kernels_per_level * kLevelsPerIteration * iters);
+  }
   return MG_OK;
 }
 
