@@ -15,6 +15,11 @@
 // Only push levels are run, because the in-edges a pull level reads would need
 // a transpose the caller may not have.
 //
+// Under CUDA's lazy module loading (the default) the first call on a device
+// may be the moment the driver loads this module and backs the array, so a
+// caller that reserves nearly all device memory for its own pool should make
+// one call (any small graph) before reserving.
+//
 // The array is shared by every call on a device and keeps the last call's
 // contents; the bitmaps that must start cleared are cleared by each call, and
 // the look-back epoch carried in the control block keeps stale status words
@@ -187,6 +192,10 @@ extern "C" int mg_bfs_noalloc(const int32_t *d_row_offsets, const int32_t *d_col
     stats->push_iterations = (int32_t)hc.push_levels;
     stats->converged = hc.frontier_size == 0 ? 1 : 0;
     stats->vertices_reached = (int64_t)hc.visited_count;
+    // out-degrees of the reached vertices, summed level by level on the device
+    // (the same count mg_bfs reports); device_ms stays 0: timing events are
+    // driver resources this entry point does not create
+    stats->edges_traversed = (int64_t)hc.visited_edges;
   }
   return MG_OK;
 }

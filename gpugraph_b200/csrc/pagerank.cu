@@ -266,6 +266,16 @@ __global__ void k_pr_level_end(Ctl *ctl, double damping, double inv_n, double to
   if (use_handle) cudaGraphSetConditional(h, ctl->active);
 }
 
+// Control block of a PageRank run, with the base term of the first iteration
+// (passed by value, so no host buffer has to outlive the launch).
+__global__ void k_pr_ctl_init(Ctl *ctl, uint32_t max_iter, unsigned long long spin_limit, uint32_t flags,
+                              double base0) {
+  if (threadIdx.x == 0) {
+    ctl_init_body(ctl, 1u, max_iter, spin_limit, MODE_QUEUE, flags);
+    ctl->dangling = base0;
+  }
+}
+
 __global__ void k_pr_init(const float *inv, float *r, float *c, int32_t V, float r0) {
   for (int64_t v = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; v < V; v += (int64_t)gridDim.x * blockDim.x) {
     r[v] = r0;
@@ -444,11 +454,10 @@ extern "C" int mg_pagerank(mg_graph *g, float *ranks, mg_stats *stats, const mg_
   a.damping = (float)d;
   a.ctl = g->ws.ctl;
   k_pr_init<<<g->num_sms * 4, 256, 0, s>>>(a.inv, a.r0, a.c0, V, (float)inv_n);
-  k_ctl_init<<<1, 32, 0, s>>>(a.ctl, 1u, max_iter, (unsigned long long)o->spin_limit, MODE_QUEUE, ctl_flags(nullptr));
-  count_launch(2);
   const double base0 = (1.0 - d) * inv_n + d * ((double)g->pr_ndangling * inv_n) * inv_n;
-  cudaError_t e = cudaMemcpyAsync(&a.ctl->dangling, &base0, sizeof(double), cudaMemcpyHostToDevice, s);
-  if ((st = cuda_status(e, "pagerank init")) != MG_OK) return st;
+  k_pr_ctl_init<<<1, 32, 0, s>>>(a.ctl, max_iter, (unsigned long long)o->spin_limit, ctl_flags(nullptr), base0);
+  count_launch(2);
+  if ((st = launch_check("pagerank init")) != MG_OK) return st;
   const int grid = persistent_grid(g, o, 6);  // 48 warps per SM (40 registers per thread)
   const int fix_grid = std::max(1, std::min(g->num_sms * 4, (g->pr_nheavy + kNT - 1) / kNT));
   const double tol = o->tolerance;

@@ -214,8 +214,13 @@ int mg_ppr_backward(mg_graph *g, const float *edge_weights, const float *ranks,
  * lives in one static device array of about 14 MiB per GPU, so the call itself
  * allocates nothing. Limits: nodes <= 2^20, edges <= 2^24 (MG_ERR_ARG beyond).
  * Runs push levels only; results equal mg_bfs. The first call on a device looks
- * up the array's device address, so make it before any stream capture. Calls
+ * up the array's device address, so make it before any stream capture; under
+ * CUDA's lazy module loading that first call may also be when the driver loads
+ * the module and backs the array, so a caller about to reserve nearly all
+ * device memory for its own pool should make one call before reserving. Calls
  * share the array: calls that overlap on the GPU race and must be serialised.
+ * stats (may be NULL): iterations, vertices_reached and edges_traversed as
+ * mg_bfs reports them; device_ms is 0 (no timing events are created).
  * stream may be NULL (legacy default stream). */
 int mg_bfs_noalloc(const int32_t *d_row_offsets, const int32_t *d_column_indices, int64_t nodes,
                    int64_t edges, int32_t src, int32_t *d_depths, void *stream, mg_stats *stats);

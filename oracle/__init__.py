@@ -41,6 +41,10 @@ def _load():
     lib.oracle_pr_gas.argtypes = [_I64, _P, _P, _P, _P, _P, C.c_float, C.c_int32, _P, _P]
     lib.oracle_pagerank_fp64.argtypes = [_I64, _P, _P, _P, C.c_double, C.c_double, C.c_int32, _P, _P, _P]
     lib.oracle_bfs_pred.argtypes = [_I64, _P, _P, _P, _P]
+    lib.oracle_build_rmat.argtypes = [C.c_int32, C.c_int32, C.c_double, C.c_double, C.c_double, C.c_uint64,
+                                      C.c_int32, C.c_int32, C.POINTER(C.POINTER(C.c_int32)),
+                                      C.POINTER(C.POINTER(C.c_int32)), C.POINTER(_I64)]
+    lib.oracle_free.argtypes = [_P]
     return lib
 
 
@@ -125,6 +129,22 @@ def pagerank_fp64(ro, coff, crow, damping=0.85, tol=1e-6, max_iter=100):
     assert lib().oracle_pagerank_fp64(len(ro) - 1, _p(ro), _p(coff), _p(crow), damping, tol, max_iter, _p(out),
                                       C.byref(it), C.byref(res)) == 0
     return out, it.value, res.value
+
+
+def rmat(scale, edgefactor=16, seed=1, symmetrize=True, a=0.57, b=0.19, c=0.19):
+    """Seeded R-MAT CSR (row_offsets, column_indices) built without the product
+    library: the same bytes as gpugraph_b200.HostGraph.rmat (asserted by tests)."""
+    ro_p, col_p, m = C.POINTER(C.c_int32)(), C.POINTER(C.c_int32)(), _I64(0)
+    assert lib().oracle_build_rmat(scale, edgefactor, a, b, c, seed, int(symmetrize), 1, C.byref(ro_p),
+                                   C.byref(col_p), C.byref(m)) == 0
+    n = 1 << scale
+    try:
+        ro = np.ctypeslib.as_array(ro_p, shape=(n + 1,)).copy()
+        col = np.ctypeslib.as_array(col_p, shape=(max(m.value, 1),))[:m.value].copy()
+    finally:
+        lib().oracle_free(C.cast(ro_p, _P))
+        lib().oracle_free(C.cast(col_p, _P))
+    return ro, col
 
 
 # --------------------------------------------------- reference functions --

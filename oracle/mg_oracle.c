@@ -285,3 +285,138 @@ int oracle_bfs_pred(int64_t n, const int32_t *coff, const int32_t *crow, const i
   }
   return 0;
 }
+
+/* Seeded R-MAT input generator: a plain-C restatement of the product library's
+ * host builder (mg_build_rmat: recursive quadrant choice as in the reference's
+ * BuildRmatGraph, b40c/graph/builder/rmat.cuh:145-224, with counter-hash draws,
+ * no per-level jitter and a seeded vertex relabelling; then a CSR with sorted
+ * rows, optionally symmetrised, self-loops and duplicates dropped). It exists so
+ * that the reference CPU baseline builds its input without loading the product
+ * library; tests assert the two CSRs are byte-identical. Draw (seed, stream,
+ * index) -> 64 bits: splitmix64 of splitmix64(seed ^ stream*K) ^ index. */
+static uint64_t om_splitmix(uint64_t x) {
+  x += 0x9E3779B97F4A7C15ull;
+  x = (x ^ (x >> 30)) * 0xBF58476D1CE4E5B9ull;
+  x = (x ^ (x >> 27)) * 0x94D049BB133111EBull;
+  return x ^ (x >> 31);
+}
+static uint64_t om_hash3(uint64_t seed, uint64_t stream, uint64_t idx) {
+  return om_splitmix(om_splitmix(seed ^ (stream * 0xD1B54A32D192ED03ull)) ^ idx);
+}
+/* ascending sort of ids: quicksort (median of three) down to runs of 16, then
+ * insertion sort */
+static void om_sort_ids(int32_t *p, int64_t d) {
+  while (d > 16) {
+    int32_t x = p[0], y = p[d / 2], z = p[d - 1], piv;
+    piv = x < y ? (y < z ? y : (x < z ? z : x)) : (x < z ? x : (y < z ? z : y));
+    int64_t i = 0, j = d - 1;
+    for (;;) {
+      while (p[i] < piv) ++i;
+      while (p[j] > piv) --j;
+      if (i >= j) break;
+      const int32_t t = p[i];
+      p[i++] = p[j];
+      p[j--] = t;
+    }
+    /* recurse into the smaller side, loop on the larger */
+    if (j + 1 < d - j - 1) {
+      om_sort_ids(p, j + 1);
+      p += j + 1;
+      d -= j + 1;
+    } else {
+      om_sort_ids(p + j + 1, d - j - 1);
+      d = j + 1;
+    }
+  }
+  for (int64_t i = 1; i < d; ++i) {
+    const int32_t x = p[i];
+    int64_t k = i;
+    while (k > 0 && p[k - 1] > x) {
+      p[k] = p[k - 1];
+      --k;
+    }
+    p[k] = x;
+  }
+}
+
+/* On success *ro_out (n+1 entries) and *col_out (*edges_out entries) are
+ * malloc'd; release them with oracle_free. */
+int oracle_build_rmat(int32_t scale, int32_t edgefactor, double a, double b, double c, uint64_t seed,
+                      int32_t symmetrize, int32_t clean, int32_t **ro_out, int32_t **col_out, int64_t *edges_out) {
+  if (scale < 1 || scale > 30 || edgefactor < 1) return -1;
+  const int64_t n = (int64_t)1 << scale, m = (int64_t)edgefactor * n;
+  const double s32 = 4294967296.0;
+  const uint64_t tA = (uint64_t)(a * s32), tAB = (uint64_t)((a + b) * s32), tABC = (uint64_t)((a + b + c) * s32);
+  int32_t *perm = (int32_t *)malloc(sizeof(int32_t) * (size_t)n);
+  int32_t *src = (int32_t *)malloc(sizeof(int32_t) * (size_t)m), *dst = (int32_t *)malloc(sizeof(int32_t) * (size_t)m);
+  int64_t *off = (int64_t *)calloc((size_t)n + 1, sizeof(int64_t));
+  if (!perm || !src || !dst || !off) return -1;
+  for (int64_t i = 0; i < n; ++i) perm[i] = (int32_t)i;
+  for (int64_t i = n - 1; i > 0; --i) { /* Fisher-Yates over the counter hash */
+    const uint64_t r = om_hash3(seed, 0x7065726dull, (uint64_t)i) % (uint64_t)(i + 1);
+    const int32_t t = perm[i];
+    perm[i] = perm[r];
+    perm[r] = t;
+  }
+  for (int64_t k = 0; k < m; ++k) {
+    uint32_t u = 0, v = 0;
+    uint64_t h = 0;
+    for (int lvl = 0; lvl < scale; ++lvl) {
+      if ((lvl & 1) == 0) h = om_hash3(seed, 0x726d6174ull + (uint64_t)(lvl >> 1), (uint64_t)k);
+      const uint64_t r = (lvl & 1) ? (h >> 32) : (h & 0xffffffffull);
+      const uint32_t bu = r >= tAB, bv = (r >= tA && r < tAB) || r >= tABC;
+      u = (u << 1) | bu;
+      v = (v << 1) | bv;
+    }
+    src[k] = perm[u];
+    dst[k] = perm[v];
+  }
+  free(perm);
+  for (int64_t k = 0; k < m; ++k) {
+    if (clean && src[k] == dst[k]) continue;
+    ++off[src[k] + 1];
+    if (symmetrize) ++off[dst[k] + 1];
+  }
+  for (int64_t v = 0; v < n; ++v) off[v + 1] += off[v];
+  int32_t *tmp = (int32_t *)malloc(sizeof(int32_t) * (size_t)(off[n] > 0 ? off[n] : 1));
+  int64_t *cur = (int64_t *)malloc(sizeof(int64_t) * (size_t)n);
+  if (!tmp || !cur) return -1;
+  memcpy(cur, off, sizeof(int64_t) * (size_t)n);
+  for (int64_t k = 0; k < m; ++k) {
+    if (clean && src[k] == dst[k]) continue;
+    tmp[cur[src[k]]++] = dst[k];
+    if (symmetrize) tmp[cur[dst[k]]++] = src[k];
+  }
+  free(src);
+  free(dst);
+  /* sort every row, drop duplicates; cur[v] becomes the kept length */
+  for (int64_t v = 0; v < n; ++v) {
+    int32_t *p = tmp + off[v];
+    const int64_t d = off[v + 1] - off[v];
+    om_sort_ids(p, d);
+    int64_t k = d;
+    if (clean && d > 1) {
+      k = 1;
+      for (int64_t i = 1; i < d; ++i)
+        if (p[i] != p[k - 1]) p[k++] = p[i];
+    }
+    cur[v] = k;
+  }
+  int32_t *ro = (int32_t *)malloc(sizeof(int32_t) * (size_t)(n + 1));
+  int64_t total = 0;
+  for (int64_t v = 0; v < n; ++v) total += cur[v];
+  int32_t *col = (int32_t *)malloc(sizeof(int32_t) * (size_t)(total > 0 ? total : 1));
+  if (!ro || !col) return -1;
+  ro[0] = 0;
+  for (int64_t v = 0; v < n; ++v) ro[v + 1] = ro[v] + (int32_t)cur[v];
+  for (int64_t v = 0; v < n; ++v) memcpy(col + ro[v], tmp + off[v], sizeof(int32_t) * (size_t)cur[v]);
+  free(tmp);
+  free(cur);
+  free(off);
+  *ro_out = ro;
+  *col_out = col;
+  *edges_out = total;
+  return 0;
+}
+
+void oracle_free(void *p) { free(p); }

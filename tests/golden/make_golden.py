@@ -1,9 +1,9 @@
 """Generates tests/golden/*.json from the reference's own CPU functions.
 
 Run in a checkout where the reference tree is present (oracle/_ref is built
-from it by oracle/build_ref.sh):
+from it by oracle/build_ref.sh; both read its location from $MG_REFERENCE):
 
-    python tests/golden/make_golden.py
+    MG_REFERENCE=<reference checkout> python tests/golden/make_golden.py
 
 Each fixture stores a small graph (derived CSR arrays, not the reference's
 files) together with the outputs of CPUBFS / CPUSSSP / CPUCC / CPUPR on it, so
@@ -15,6 +15,7 @@ from __future__ import annotations
 
 import hashlib
 import json
+import os
 import sys
 from pathlib import Path
 
@@ -27,7 +28,8 @@ import oracle  # noqa: E402
 from gpugraph_b200 import HostGraph  # noqa: E402
 
 OUT = Path(__file__).resolve().parent
-REF_GRAPHS = Path("/root/reference/smallRegressionGraphs")
+# the reference checkout: $MG_REFERENCE, as for oracle/build_ref.sh
+REF_GRAPHS = Path(os.environ.get("MG_REFERENCE", "/root/reference")) / "smallRegressionGraphs"
 
 
 def csr_sha(g: HostGraph) -> str:
