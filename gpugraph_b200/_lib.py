@@ -147,7 +147,7 @@ def check(status: int, where: str) -> None:
 def profile_read() -> dict:
     """Per-kernel profile accumulated since mg_profile_enable(1): name -> (ms, launches, bytes)."""
     out = {}
-    for k in range(12):
+    for k in range(13):
         name, ms, n, b = C.c_char_p(), C.c_double(), C.c_int64(), C.c_uint64()
         check(lib.mg_profile_read(k, C.byref(name), C.byref(ms), C.byref(n), C.byref(b)), "mg_profile_read")
         if n.value:

@@ -69,11 +69,17 @@ __global__ void __launch_bounds__(kNT) k_cc_sample(const int32_t *ro, const int3
                                                    int r, Ctl *ctl) {
   const unsigned long long limit = ctl->spin_limit;
   bool ok = true;
+  unsigned long long my_bytes = 0;
   for (int v = blockIdx.x * blockDim.x + threadIdx.x; v < V; v += gridDim.x * blockDim.x) {
     const int e = ro[v] + r;
-    if (e < ro[v + 1] && !cc_unite(parent, v, col[e], limit)) ok = false;
+    my_bytes += 8;  // two offsets
+    if (e < ro[v + 1]) {
+      my_bytes += 12;  // the neighbour id, the two parents read by the link
+      if (!cc_unite(parent, v, col[e], limit)) ok = false;
+    }
   }
   if (!ok) raise_error(ctl, MG_ERR_TIMEOUT);
+  add_bytes(ctl, KID_CC, my_bytes);
 }
 
 // Step 2: the root held by most of kCcProbe fixed sample vertices (ties: the
@@ -150,15 +156,18 @@ __global__ void __launch_bounds__(kNT) k_cc_rest(const int32_t *ro, const int32_
     }
   }
   if (!ok) raise_error(ctl, MG_ERR_TIMEOUT);
-  add_bytes(ctl, KID_OTHER, my_bytes);
+  add_bytes(ctl, KID_CC, my_bytes);
 }
 
 // Final labels: every vertex's root (the smallest id of its component).
-__global__ void __launch_bounds__(kNT) k_cc_flatten(int32_t *parent, int32_t V) {
+__global__ void __launch_bounds__(kNT) k_cc_flatten(int32_t *parent, int32_t V, Ctl *ctl) {
+  unsigned long long my_bytes = 0;
   for (int v = blockIdx.x * blockDim.x + threadIdx.x; v < V; v += gridDim.x * blockDim.x) {
     const int r = cc_find(parent, v);
     parent[v] = r;
+    my_bytes += 12;  // the vertex's parent, its root's parent, the write
   }
+  add_bytes(ctl, KID_CC, my_bytes);
 }
 
 // Union-find CC on a symmetric graph (called by mg_cc).
@@ -174,21 +183,22 @@ int cc_union_find(mg_graph *g, int32_t *labels, mg_stats *stats, const mg_option
   if (e != cudaSuccess) return cuda_status(e, "event record");
   int32_t *giant = reinterpret_cast<int32_t *>(g->ws.scan);  // scratch word (the scan buffer is free here)
   const int vgrid = g->num_sms * 8;
-  k_sequence_i32<<<g->num_sms * 4, 256, 0, s>>>(parent, V);
+  MG_LAUNCH(KID_CC, s, (k_sequence_i32<<<g->num_sms * 4, 256, 0, s>>>(parent, V)));
   k_ctl_init<<<1, 32, 0, s>>>(ctl, 1u, 1u, (unsigned long long)o->spin_limit, MODE_QUEUE, ctl_flags(nullptr));
   for (int r = 0; r < kCcSample; ++r) {
-    k_cc_sample<<<vgrid, kNT, 0, s>>>(g->csr.row_offsets, g->csr.col, parent, V, r, ctl);
-    k_cc_flatten<<<vgrid, kNT, 0, s>>>(parent, V);
+    MG_LAUNCH(KID_CC, s, (k_cc_sample<<<vgrid, kNT, 0, s>>>(g->csr.row_offsets, g->csr.col, parent, V, r, ctl)));
+    MG_LAUNCH(KID_CC, s, (k_cc_flatten<<<vgrid, kNT, 0, s>>>(parent, V, ctl)));
   }
-  k_cc_giant<<<1, kCcProbe, 0, s>>>(parent, V, giant);
-  k_cc_rest<<<vgrid, kNT, 0, s>>>(g->csr.row_offsets, g->csr.col, parent, V, giant, ctl);
-  k_cc_flatten<<<vgrid, kNT, 0, s>>>(parent, V);
+  MG_LAUNCH(KID_CC, s, (k_cc_giant<<<1, kCcProbe, 0, s>>>(parent, V, giant)));
+  MG_LAUNCH(KID_CC, s, (k_cc_rest<<<vgrid, kNT, 0, s>>>(g->csr.row_offsets, g->csr.col, parent, V, giant, ctl)));
+  MG_LAUNCH(KID_CC, s, (k_cc_flatten<<<vgrid, kNT, 0, s>>>(parent, V, ctl)));
   count_launch(5 + 2 * kCcSample);
   if ((st = launch_check("cc union-find")) != MG_OK) return st;
   e = cudaEventRecord(g->ev1, s);
   if (e != cudaSuccess) return cuda_status(e, "event record");
   Ctl c;
   if ((st = read_ctl(g, s, &c)) != MG_OK) return st;
+  prof_flush(s, c.kbytes);
   if (c.error) return set_error(c.error, std::string("cc: device reported ") + mg_status_string(c.error));
   float ms = 0.f;
   cudaEventElapsedTime(&ms, g->ev0, g->ev1);

@@ -57,7 +57,7 @@ struct Ctl {
   double acc[4];            // FP64 reduction slots
   // Algorithmic bytes moved by each kernel kind over the run (element-granular
   // reads and writes the algorithm needs; see KernelId).
-  unsigned long long kbytes[12];
+  unsigned long long kbytes[13];
 };
 
 // Kernel kinds for per-kernel byte accounting and profiling.
@@ -73,8 +73,10 @@ enum KernelId : int {
   KID_GATHER = 8,
   KID_APPLY = 9,
   KID_PPR = 10,
-  KID_OTHER = 11
+  KID_CC = 11,
+  KID_OTHER = 12
 };
+constexpr int kNumKernelKinds = 13;
 
 // Adds a warp's byte count to the run's counter for kernel kind `kid` (one
 // atomic per warp; call from every thread with its own count). Only while

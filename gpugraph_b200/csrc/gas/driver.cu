@@ -22,17 +22,19 @@ int read_ctl(mg_graph *g, cudaStream_t s, Ctl *out) {
 
 // ---------------------------------------------------------------- profiler --
 namespace {
-const char *kKernelNames[12] = {"frontier_scan", "expand_contract", "bfs_pull",    "multi_bfs_pull",
-                                "multi_bfs_apply", "frontier_convert", "multi_sssp_expand", "pagerank_pull",
-                                "gather",          "apply",           "ppr",               "other"};
+const char *kKernelNames[kNumKernelKinds] = {"frontier_scan",   "expand_contract", "bfs_pull",
+                                             "multi_bfs_pull",  "multi_bfs_apply", "frontier_convert",
+                                             "multi_sssp_expand", "pagerank_pull", "gather",
+                                             "apply",           "ppr",             "cc",
+                                             "other"};
 struct Profiler {
   bool on = false;
   std::vector<std::pair<int, cudaEvent_t>> marks;
   std::vector<cudaEvent_t> pool;
   size_t used = 0;
-  double ms[12] = {0};
-  int64_t launches[12] = {0};
-  unsigned long long bytes[12] = {0};
+  double ms[kNumKernelKinds] = {0};
+  int64_t launches[kNumKernelKinds] = {0};
+  unsigned long long bytes[kNumKernelKinds] = {0};
   cudaEvent_t next_event() {
     if (used == pool.size()) {
       cudaEvent_t e;
@@ -71,7 +73,7 @@ void prof_flush(cudaStream_t s, const unsigned long long *kbytes) {
   g_prof.marks.clear();
   g_prof.used = 0;
   if (kbytes)
-    for (int k = 0; k < 12; ++k) g_prof.bytes[k] += kbytes[k];
+    for (int k = 0; k < kNumKernelKinds; ++k) g_prof.bytes[k] += kbytes[k];
 }
 
 int prepare_run(mg_graph *g, cudaStream_t s) {
@@ -202,7 +204,7 @@ int mg_profile_enable(int enable) {
   mg::g_prof.on = enable != 0;
   mg::g_prof.marks.clear();
   mg::g_prof.used = 0;
-  for (int k = 0; k < 12; ++k) {
+  for (int k = 0; k < mg::kNumKernelKinds; ++k) {
     mg::g_prof.ms[k] = 0;
     mg::g_prof.launches[k] = 0;
     mg::g_prof.bytes[k] = 0;
@@ -211,7 +213,7 @@ int mg_profile_enable(int enable) {
 }
 
 int mg_profile_read(int32_t kind, const char **name, double *total_ms, int64_t *launches, uint64_t *bytes) {
-  if (kind < 0 || kind >= 12) return mg::set_error(MG_ERR_ARG, "kernel kind out of range");
+  if (kind < 0 || kind >= mg::kNumKernelKinds) return mg::set_error(MG_ERR_ARG, "kernel kind out of range");
   if (name) *name = mg::kKernelNames[kind];
   if (total_ms) *total_ms = mg::g_prof.ms[kind];
   if (launches) *launches = mg::g_prof.launches[kind];

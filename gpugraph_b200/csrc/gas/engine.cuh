@@ -76,7 +76,10 @@ struct GasArgs {
   typename P::GatherType *gather_tmp;  // contract scratch / apply input
   typename P::GatherType *gather_res;  // gather phase output
   Ctl *ctl;
-  int32_t expand_in;  // 1: expand over the transpose (EXPAND_IN_EDGES)
+  // 0: expand over the out-edges (EXPAND_OUT_EDGES), 1: over the in-edges of the
+  // transpose (EXPAND_IN_EDGES), 2: over both (EXPAND_ALL_EDGES; a vertex's items
+  // are its out-edges, then its in-edges)
+  int32_t expand_in;
   int32_t gather_dir; // GatherEdges value
 };
 
@@ -185,7 +188,8 @@ __global__ void __launch_bounds__(kNT) k_frontier_scan(GasArgs<P> a) {
   const unsigned long long spin_limit = ctl->spin_limit;
   const int32_t *F = cur_queue(a, level);
   uint32_t *clear_bm = cur_bm(a, level);
-  const int32_t *ro = a.expand_in ? a.g.csc_offsets : a.g.row_offsets;
+  const int32_t *ro = a.expand_in == 1 ? a.g.csc_offsets : a.g.row_offsets;
+  const bool both = a.expand_in == 2;
   const uint32_t ntiles = (n + TV - 1) / TV;
   typename P::expand_vertex ev;
   unsigned long long my_bytes = 0;
@@ -206,6 +210,7 @@ __global__ void __launch_bounds__(kNT) k_frontier_scan(GasArgs<P> a) {
         bool expand = true;
         if (skip_unchanged_trait<P>::value) expand = ev(v, (char)a.changed[v], a.vl, a.el);
         d = expand ? (uint32_t)(ro[v + 1] - ro[v]) : 0u;
+        if (expand && both) d += (uint32_t)(a.g.csc_offsets[v + 1] - a.g.csc_offsets[v]);
       }
       deg[k] = d;
       tsum += d;
@@ -391,8 +396,9 @@ __global__ void __launch_bounds__(kNT) k_expand(GasArgs<P> a) {
   const int32_t *F = cur_queue(a, level);
   int32_t *Fout = nxt_queue(a, level);
   uint32_t *dedup = nxt_bm(a, level);
-  const int32_t *ro = a.expand_in ? a.g.csc_offsets : a.g.row_offsets;
-  const int32_t *nb = a.expand_in ? a.g.csc_rows : a.g.col;
+  const int32_t *ro = a.expand_in == 1 ? a.g.csc_offsets : a.g.row_offsets;
+  const int32_t *nb = a.expand_in == 1 ? a.g.csc_rows : a.g.col;
+  const bool both = a.expand_in == 2;
   const int32_t V = a.g.V;
   typename P::expand_vertex ev;
   typename P::expand_edge ee;
@@ -432,10 +438,20 @@ __global__ void __launch_bounds__(kNT) k_expand(GasArgs<P> a) {
         my_bytes += (el >= 0) ? (unsigned long long)(4 + probe_bytes_trait<P>::value) : 12ull;
         if (el >= 0) {
           const int v = s_v[j];
-          const int eid = s_rs[j] + el;
+          int eid = s_rs[j] + el;
+          const int32_t *nbp = nb;
+          bool in_edge = a.expand_in == 1;
+          if (both) {  // past the out-edges: the in-edges of v
+            const int od = ro[v + 1] - s_rs[j];
+            if (el >= od) {
+              eid = a.g.csc_offsets[v] + (el - od);
+              nbp = a.g.csc_rows;
+              in_edge = true;
+            }
+          }
           if ((unsigned)eid < (unsigned)a.g.E) {
-            const int nbr = nb[eid];
-            const int eidv = (a.expand_in && a.g.csc_eid) ? a.g.csc_eid[eid] : eid;
+            const int nbr = nbp[eid];
+            const int eidv = (in_edge && a.g.csc_eid) ? a.g.csc_eid[eid] : eid;
             typename P::MiscType misc = typename P::MiscType();
             ee(s_ch[j] != 0, (int)level, v, nbr, eidv, a.vl, a.el, fo, misc);
             if (fo >= V) {
@@ -455,7 +471,10 @@ __global__ void __launch_bounds__(kNT) k_expand(GasArgs<P> a) {
             uint32_t *w = dedup + (fo >> 5);
             if (!(ld_volatile(w) & bit)) surv = !(atomicOr(w, bit) & bit);
           }
-          if (track_next_edges_trait<P>::value && surv) my_edges += (unsigned long long)(ro[fo + 1] - ro[fo]);
+          if (track_next_edges_trait<P>::value && surv) {
+            my_edges += (unsigned long long)(ro[fo + 1] - ro[fo]);
+            if (both) my_edges += (unsigned long long)(a.g.csc_offsets[fo + 1] - a.g.csc_offsets[fo]);
+          }
         }
       }
       bal[r] = __ballot_sync(0xffffffffu, surv);

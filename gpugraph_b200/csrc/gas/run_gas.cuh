@@ -40,7 +40,7 @@ GasArgs<P> base_args(mg_graph *g) {
   a.gather_tmp = reinterpret_cast<typename P::GatherType *>(w.gather_tmp);
   a.gather_res = reinterpret_cast<typename P::GatherType *>(w.vbuf[1]);
   a.ctl = w.ctl;
-  a.expand_in = (P::expandOverEdges() == EXPAND_IN_EDGES) ? 1 : 0;
+  a.expand_in = P::expandOverEdges() == EXPAND_IN_EDGES ? 1 : P::expandOverEdges() == EXPAND_ALL_EDGES ? 2 : 0;
   a.gather_dir = (int32_t)P::gatherOverEdges();
   return a;
 }
@@ -49,9 +49,8 @@ GasArgs<P> base_args(mg_graph *g) {
 // expand/contract -> level end. n0 = initial frontier size (already in queue 0).
 template <class P>
 int run_gas(mg_graph *g, const GasArgs<P> &a, uint32_t n0, const mg_options *o, const char *name, LoopResult *res) {
-  // EXPAND_ALL_EDGES has no engine path; NO_EXPAND_EDGES ends the run after one
-  // gather/apply round (nothing enters the next frontier).
-  if (P::expandOverEdges() == EXPAND_ALL_EDGES) return set_error(MG_ERR_UNSUPPORTED, "EXPAND_ALL_EDGES");
+  // NO_EXPAND_EDGES ends the run after one gather/apply round (nothing enters
+  // the next frontier); EXPAND_ALL_EDGES expands out-edges and in-edges.
   cudaStream_t s = run_stream(g, o);
   const int grid = persistent_grid(g, o, 4);
   // Every level of a traversal settles at least one vertex, so V + 2 levels bound

@@ -8,8 +8,12 @@
 // HBM layout (per graph, allocated on first use):
 //   mask[0]      visit[V]   u64: bit s set once source s has reached v (BFS)
 //   mask[1..2]   F[2][V]    u64: level-parity frontier masks
-//   multi_out    [V][64]    int32 per-source results (256 contiguous bytes per vertex)
-// Results are transposed to the caller's [nsrc][V] layout at the end.
+//   multi_out    [V][64]    per-source results: uint16 BFS depths (128 contiguous
+//                           bytes per vertex), or int32 SSSP distances (256 bytes)
+// Results are transposed to the caller's int32 [nsrc][V] layout at the end. A
+// batched BFS keeps 16-bit depths, which halves the bytes of the scattered
+// depth writes and of the transpose's reads; a run that would pass level
+// 65534 stops there and is rerun with int32 depth rows.
 //
 // BFS levels switch between push (the GAS engine's load-balanced expand with
 // an OR-into-mask Program, next frontier as a vertex queue) and pull (every
@@ -91,7 +95,7 @@ struct msbfs_push {
 struct MultiArgs {
   DevCsr g;
   u64 *visit, *F0, *F1;
-  int32_t *out;  // [V][64]
+  int32_t *out;  // [V][64]: int32 rows, or uint16 rows (batched BFS; see depth_rows)
   int32_t *q0, *q1;
   uint32_t *bm0, *bm1;
   unsigned long long *status;
@@ -100,6 +104,11 @@ struct MultiArgs {
 };
 
 MG_DEVINL u64 *cur_F(const MultiArgs &a, uint32_t L) { return (L & 1) ? a.F1 : a.F0; }
+// The [V][64] result rows seen as DT (uint16_t or int32_t depths).
+template <typename DT>
+MG_DEVINL DT *depth_rows(const MultiArgs &a) { return reinterpret_cast<DT *>(a.out); }
+// Levels a uint16 depth row can hold (depth 65535 is never written).
+constexpr uint32_t kMsDepth16Levels = 65534;
 MG_DEVINL u64 *nxt_F(const MultiArgs &a, uint32_t L) { return (L & 1) ? a.F0 : a.F1; }
 MG_DEVINL int32_t *cur_Q(const MultiArgs &a, uint32_t L) { return (L & 1) ? a.q1 : a.q0; }
 MG_DEVINL int32_t *nxt_Q(const MultiArgs &a, uint32_t L) { return (L & 1) ? a.q0 : a.q1; }
@@ -116,13 +125,15 @@ struct SrcList {
 };
 
 // Level-0 state of a batched run (one CTA of 64 threads).
+// bfs: 0 = SSSP (int32 rows), 1 = BFS with int32 depth rows, 2 = BFS with uint16 rows.
 __global__ void k_ms_init(MultiArgs a, SrcList L, int bfs) {
   const int t = threadIdx.x;
   if (t < L.nsrc) {
     const int v = L.src[t];
     atomicOr(&a.F0[v], 1ull << t);
     if (bfs) atomicOr(&a.visit[v], 1ull << t);
-    a.out[(int64_t)v * 64 + t] = 0;
+    if (bfs == 2) depth_rows<uint16_t>(a)[(int64_t)v * 64 + t] = 0;
+    else a.out[(int64_t)v * 64 + t] = 0;
   }
   if (t < L.ndistinct) a.q0[t] = L.distinct[t];
   if (t == 0 && bfs) {
@@ -136,6 +147,7 @@ __global__ void k_ms_init(MultiArgs a, SrcList L, int bfs) {
 
 // Start of a level after a push level: the queued vertices keep only their
 // new sources (depth = level), and the previous level's masks are cleared.
+template <typename DT>
 __global__ void __launch_bounds__(kNT) k_ms_apply(MultiArgs a) {
   Ctl *ctl = a.ctl;
   if (!ctl->active || !ctl->apply_pending) return;
@@ -160,7 +172,7 @@ __global__ void __launch_bounds__(kNT) k_ms_apply(MultiArgs a) {
       my_bytes += 28;  // queue entry, visit and mask read, mask write
       if (nb) {
         a.visit[v] = vis | nb;
-        my_bytes += 8 + 4ull * (unsigned long long)__popcll(nb);
+        my_bytes += 8 + sizeof(DT) * (unsigned long long)__popcll(nb);
       }
     }
     uint32_t wv = __ballot_sync(0xffffffffu, nb != 0);
@@ -168,9 +180,9 @@ __global__ void __launch_bounds__(kNT) k_ms_apply(MultiArgs a) {
       const int j = __ffs(wv) - 1;
       wv &= wv - 1;
       const u64 m = __shfl_sync(0xffffffffu, nb, j);
-      int32_t *row = a.out + (int64_t)__shfl_sync(0xffffffffu, v, j) * 64;
-      if ((m >> lane) & 1ull) row[lane] = (int32_t)L;
-      if ((m >> (lane + 32)) & 1ull) row[lane + 32] = (int32_t)L;
+      DT *row = depth_rows<DT>(a) + (int64_t)__shfl_sync(0xffffffffu, v, j) * 64;
+      if ((m >> lane) & 1ull) row[lane] = (DT)L;
+      if ((m >> (lane + 32)) & 1ull) row[lane + 32] = (DT)L;
     }
   }
   for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < pn; i += gridDim.x * blockDim.x) {
@@ -236,6 +248,7 @@ MG_DEVINL void ms_segment(u64 x, int ck, int b, int e, bool starts, bool take, u
 // granularity while the loads stay coalesced and balanced across lanes. The
 // new depths of a vertex are written by the whole warp (lane l: sources l and
 // l+32 of its 256-byte row).
+template <typename DT>
 __global__ void __launch_bounds__(kNT, 5) k_ms_pull(MultiArgs a) {
   Ctl *ctl = a.ctl;
   if (!ctl->active || ctl->mode != MODE_BITMAP) return;
@@ -309,7 +322,7 @@ __global__ void __launch_bounds__(kNT, 5) k_ms_pull(MultiArgs a) {
     acc &= need;
     if (valid) Fn[v] = acc;
     if (acc) {
-      my_bytes += 8 + 4ull * (unsigned long long)__popcll(acc);  // visit write + depths
+      my_bytes += 8 + sizeof(DT) * (unsigned long long)__popcll(acc);  // visit write + depths
       a.visit[v] = vis | acc;
       my_cnt += 1;
       my_edges += (unsigned long long)(ro[v + 1] - ro[v]);
@@ -320,9 +333,9 @@ __global__ void __launch_bounds__(kNT, 5) k_ms_pull(MultiArgs a) {
       const int j = __ffs(wv) - 1;
       wv &= wv - 1;
       const u64 m = __shfl_sync(0xffffffffu, acc, j);
-      int32_t *row = a.out + (int64_t)(v0 + j) * 64;
-      if ((m >> lane) & 1ull) row[lane] = (int32_t)L + 1;
-      if ((m >> (lane + 32)) & 1ull) row[lane + 32] = (int32_t)L + 1;
+      DT *row = depth_rows<DT>(a) + (int64_t)(v0 + j) * 64;
+      if ((m >> lane) & 1ull) row[lane] = (DT)(L + 1);
+      if ((m >> (lane + 32)) & 1ull) row[lane + 32] = (DT)(L + 1);
     }
   }
   add_bytes(ctl, KID_MS_PULL, my_bytes);
@@ -446,57 +459,88 @@ __global__ void k_ms_level_end(Ctl *ctl, int32_t V, int64_t E, cudaGraphConditio
   if (use_handle) cudaGraphSetConditional(h, ctl->active);
 }
 
-// [V][64] -> [ns][V] for sources s_begin .. s_begin+ns-1. A CTA walks tiles of
-// kTrV vertices (grid-stride): 16-byte loads of the 256-byte rows into shared
-// memory, then each source's kTrV results leave as 128-byte coalesced stores;
-// the next tile's loads are in flight while the current tile is written out.
-// With `visit` given (batched BFS), an entry whose visit bit is clear is
-// unreached: it comes out as -1, and its slot, which the traversal never
-// wrote, is not read (a row with no bits set is not read at all).
+// [V][64] -> [ns][V] for sources s_begin .. s_begin+ns-1, widening uint16
+// depth rows to int32. A CTA walks tiles of kTrV vertices (grid-stride):
+// 16-byte loads of the rows into shared memory, then each source's kTrV results
+// leave as 128-byte coalesced stores; the next tile's loads are in flight while
+// the current tile is written out. With `visit` given (batched BFS), an entry
+// whose visit bit is clear is unreached: it comes out as -1, and its slot,
+// which the traversal never wrote, is not read (a 16-byte piece with no bits
+// set is not read at all).
 constexpr int kTrV = 64;
-constexpr int kTrQ = kTrV * 16 / 256;  // 16-byte row pieces per thread per tile
 
-MG_DEVINL void tr_load(const int32_t *in, const u64 *visit, int32_t V, int64_t v0, int4 (&q)[kTrQ]) {
+template <typename T>
+struct TrShape {
+  static constexpr int kPer = 16 / (int)sizeof(T);  // entries per 16-byte piece
+  static constexpr int kPieces = 64 / kPer;         // pieces per row
+  static constexpr int kQ = kTrV * kPieces / 256;   // pieces per thread per tile
+};
+
+template <typename T>
+MG_DEVINL void tr_load(const T *in, const u64 *visit, int32_t V, int64_t v0, int4 (&q)[TrShape<T>::kQ],
+                       uint32_t (&qb)[TrShape<T>::kQ]) {
+  constexpr int PER = TrShape<T>::kPer, PIECES = TrShape<T>::kPieces;
+  constexpr uint32_t FULL = (1u << PER) - 1u;
 #pragma unroll
-  for (int k = 0; k < kTrQ; ++k) {
-    const int idx = threadIdx.x + 256 * k, r = idx >> 4, c4 = idx & 15;
+  for (int k = 0; k < TrShape<T>::kQ; ++k) {
+    const int idx = threadIdx.x + 256 * k, r = idx / PIECES, c = idx % PIECES;
     const int64_t v = v0 + r;
     uint32_t bits = 0;
-    if (v < V) bits = visit ? (uint32_t)(visit[v] >> (4 * c4)) & 0xFu : 0xFu;
-    q[k] = bits ? *reinterpret_cast<const int4 *>(in + v * 64 + 4 * c4) : make_int4(-1, -1, -1, -1);
-    if (!(bits & 1u)) q[k].x = -1;
-    if (!(bits & 2u)) q[k].y = -1;
-    if (!(bits & 4u)) q[k].z = -1;
-    if (!(bits & 8u)) q[k].w = -1;
+    if (v < V) bits = visit ? (uint32_t)(visit[v] >> (PER * c)) & FULL : FULL;
+    qb[k] = bits;
+    q[k] = bits ? *reinterpret_cast<const int4 *>(in + v * 64 + PER * c) : make_int4(0, 0, 0, 0);
   }
 }
 
-__global__ void __launch_bounds__(256, 6) k_ms_transpose(const int32_t *in, const u64 *visit, int32_t *out, int32_t V,
+// entry i (< 16 / sizeof(T)) of a 16-byte piece, widened to int32
+template <typename T>
+MG_DEVINL int32_t tr_entry(const int4 &q, int i) {
+  const uint32_t w[4] = {(uint32_t)q.x, (uint32_t)q.y, (uint32_t)q.z, (uint32_t)q.w};
+  if (sizeof(T) == 4) return (int32_t)w[i];
+  return (int32_t)((w[i >> 1] >> (16 * (i & 1))) & 0xffffu);
+}
+
+template <typename T>
+__global__ void __launch_bounds__(256, 6) k_ms_transpose(const T *in, const u64 *visit, int32_t *out, int32_t V,
                                                       int32_t s_begin, int32_t ns) {
+  constexpr int PER = TrShape<T>::kPer, PIECES = TrShape<T>::kPieces, Q = TrShape<T>::kQ;
   __shared__ int32_t t[kTrV][65];
   const int64_t ntiles = ((int64_t)V + kTrV - 1) / kTrV;
   const int lane = lane_id(), warp = warp_id();
-  int4 q[kTrQ];
+  int4 q[Q];
+  uint32_t qb[Q];
   int64_t tile = blockIdx.x;
-  if (tile < ntiles) tr_load(in, visit, V, tile * kTrV, q);
+  if (tile < ntiles) tr_load<T>(in, visit, V, tile * kTrV, q, qb);
   for (; tile < ntiles; tile += gridDim.x) {
     const int64_t v0 = tile * kTrV;
     __syncthreads();  // the previous tile has been written out of t
 #pragma unroll
-    for (int k = 0; k < kTrQ; ++k) {
-      const int idx = threadIdx.x + 256 * k, r = idx >> 4, c = 4 * (idx & 15);
-      t[r][c] = q[k].x;
-      t[r][c + 1] = q[k].y;
-      t[r][c + 2] = q[k].z;
-      t[r][c + 3] = q[k].w;
+    for (int k = 0; k < Q; ++k) {
+      const int idx = threadIdx.x + 256 * k, r = idx / PIECES, c = PER * (idx % PIECES);
+#pragma unroll
+      for (int i = 0; i < PER; ++i) t[r][c + i] = ((qb[k] >> i) & 1u) ? tr_entry<T>(q[k], i) : -1;
     }
     __syncthreads();
-    if (tile + gridDim.x < ntiles) tr_load(in, visit, V, (tile + gridDim.x) * kTrV, q);
+    if (tile + gridDim.x < ntiles) tr_load<T>(in, visit, V, (tile + gridDim.x) * kTrV, q, qb);
     for (int seg = warp; seg < ns * (kTrV / 32); seg += kNW) {
       const int s = seg / (kTrV / 32), r = (seg % (kTrV / 32)) * 32 + lane;
       if (v0 + r < V) out[(int64_t)s * V + v0 + r] = t[r][s_begin + s];
     }
   }
+}
+
+// Transposes a run's [V][64] rows (uint16 depths when depth16, else int32) to
+// the caller's [nsrc][V] int32 layout on stream s.
+static void launch_transpose(mg_graph *g, bool depth16, const u64 *visit, int32_t *out, int32_t nsrc,
+                             cudaStream_t s) {
+  const int32_t V = g->csr.V;
+  const unsigned nblk = (unsigned)std::min<int64_t>((int64_t)g->num_sms * 6, ((int64_t)V + kTrV - 1) / kTrV);  // 6 CTAs fit on an SM
+  if (depth16)
+    k_ms_transpose<uint16_t><<<nblk, 256, 0, s>>>(reinterpret_cast<const uint16_t *>(g->multi_out), visit, out, V, 0,
+                                                  nsrc);
+  else
+    k_ms_transpose<int32_t><<<nblk, 256, 0, s>>>(g->multi_out, visit, out, V, 0, nsrc);
+  count_launch();
 }
 
 // Reached (vertex, source) pairs and the out-edges of their vertices, from the
@@ -542,6 +586,17 @@ __global__ void __launch_bounds__(kNT) k_mss_clear(MultiArgs a) {
   u64 *Fp = nxt_F(a, L);
   const int32_t *Qp = nxt_Q(a, L);
   for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < pn; i += gridDim.x * blockDim.x) Fp[Qp[i]] = 0;
+}
+
+// Lowers a distance entry to c (a fire-and-forget reduction: nothing waits for
+// the old value) and marks source t improved. The caller saw c below the entry
+// it loaded: if another relaxation lowered the entry further in between, the
+// mark is spurious and costs one extra expansion of (v, t) next level, but every
+// reduction that does lower an entry is marked by its own thread, so the
+// fixpoint is unchanged.
+MG_DEVINL void relax_min(int32_t *p, int32_t c, u64 &imp, int t) {
+  atomicMin(p, c);
+  imp |= 1ull << t;
 }
 
 template <int VT>
@@ -644,10 +699,23 @@ __global__ void __launch_bounds__(kNT) k_mss_expand(MultiArgs a, const uint32_t 
         if (bu >= 0) {
           const int32_t *du = a.out + (int64_t)bu * 64;
           int32_t *dv = a.out + (int64_t)bv * 64;
-          for (u64 m = bam; m; m &= m - 1) {
-            const int t = __ffsll((long long)m) - 1;
-            const int c = du[t] + bw;
-            if (c < dv[t] && atomicMin(&dv[t], c) > c) imp |= 1ull << t;
+          // four active sources per step, their row entries loaded together
+          for (u64 m = bam; m;) {
+            int t[4], du4[4], dv4[4];
+#pragma unroll
+            for (int q = 0; q < 4; ++q) {
+              t[q] = m ? __ffsll((long long)m) - 1 : -1;
+              m &= m - 1;
+            }
+#pragma unroll
+            for (int q = 0; q < 4; ++q)
+              if (t[q] >= 0) {
+                du4[q] = __ldcg(du + t[q]);
+                dv4[q] = __ldcg(dv + t[q]);
+              }
+#pragma unroll
+            for (int q = 0; q < 4; ++q)
+              if (t[q] >= 0 && du4[q] + bw < dv4[q]) relax_min(dv + t[q], du4[q] + bw, imp, t[q]);
           }
         }
         enqueue(imp != 0, bv, imp);
@@ -665,14 +733,14 @@ __global__ void __launch_bounds__(kNT) k_mss_expand(MultiArgs a, const uint32_t 
           const int4 *pu = reinterpret_cast<const int4 *>(a.out + (int64_t)u * 64 + 8 * sub);
           int32_t *dvp = a.out + (int64_t)v * 64 + 8 * sub;
           const int4 *pv = reinterpret_cast<const int4 *>(dvp);
-          const int4 u0 = pu[0], u1 = pu[1], v0 = pv[0], v1 = pv[1];
+          const int4 u0 = __ldcg(pu), u1 = __ldcg(pu + 1), v0 = __ldcg(pv), v1 = __ldcg(pv + 1);
           const int du[8] = {u0.x, u0.y, u0.z, u0.w, u1.x, u1.y, u1.z, u1.w};
           const int dv[8] = {v0.x, v0.y, v0.z, v0.w, v1.x, v1.y, v1.z, v1.w};
 #pragma unroll
           for (int t = 0; t < 8; ++t) {
-            if ((bits >> t) & 1u) {
-              const int c = du[t] + w;
-              if (c < dv[t] && atomicMin(&dvp[t], c) > c) imp |= 1u << t;
+            if (((bits >> t) & 1u) && du[t] + w < dv[t]) {
+              atomicMin(&dvp[t], du[t] + w);  // result unused: a reduction (see relax_min)
+              imp |= 1u << t;
             }
           }
         }
@@ -765,19 +833,14 @@ static int multi_prepare(mg_graph *g, const int32_t *srcs, int32_t nsrc, const m
 
 // Device output: the transpose runs as the level loop's epilogue, before the
 // control block is read back.
-static std::function<void(cudaStream_t)> transpose_epilogue(mg_graph *g, int32_t nsrc, int32_t *out, bool bfs) {
+static std::function<void(cudaStream_t)> transpose_epilogue(mg_graph *g, int32_t nsrc, int32_t *out, bool bfs,
+                                                            bool depth16) {
   const u64 *visit = bfs ? g->mask[0] : nullptr;
-  const int32_t *in = g->multi_out;
-  const int32_t V = g->csr.V;
-  const unsigned nblk = (unsigned)std::min<int64_t>((int64_t)g->num_sms * 6, ((int64_t)V + kTrV - 1) / kTrV);  // 6 CTAs fit on an SM
-  return [=](cudaStream_t ss) {
-    k_ms_transpose<<<nblk, 256, 0, ss>>>(in, visit, out, V, 0, nsrc);
-    count_launch();
-  };
+  return [=](cudaStream_t ss) { launch_transpose(g, depth16, visit, out, nsrc, ss); };
 }
 
 static int multi_finish(mg_graph *g, cudaStream_t s, int32_t nsrc, int32_t *out, int32_t unreached, mg_stats *stats,
-                        const mg_options *o, const LoopResult &res) {
+                        const mg_options *o, const LoopResult &res, bool depth16) {
   finish_run(g, res.ctl.level);
   if (res.ctl.error) return set_error(res.ctl.error, std::string("batched traversal: device reported ") +
                                                          mg_status_string(res.ctl.error));
@@ -815,12 +878,10 @@ static int multi_finish(mg_graph *g, cudaStream_t s, int32_t nsrc, int32_t *out,
     }
   }
   if (o->outputs_on_device) return MG_OK;  // transposed by the loop's epilogue
-  const unsigned nblk = (unsigned)std::min<int64_t>((int64_t)g->num_sms * 6, ((int64_t)V + kTrV - 1) / kTrV);  // 6 CTAs fit on an SM
   // Host output: transpose every source into a device staging buffer (kept for
   // later runs), then one copy to the caller.
   if (!g->multi_stage && (st = device_alloc(g, (void **)&g->multi_stage, (size_t)V * 64 * 4)) != MG_OK) return st;
-  k_ms_transpose<<<nblk, 256, 0, s>>>(g->multi_out, visit, g->multi_stage, V, 0, nsrc);
-  count_launch();
+  launch_transpose(g, depth16, visit, g->multi_stage, nsrc, s);
   cudaError_t e = cudaMemcpyAsync(out, g->multi_stage, (size_t)nsrc * V * 4, cudaMemcpyDeviceToHost, s);
   if (e == cudaSuccess) e = cudaStreamSynchronize(s);
   return cuda_status(e, "batched result copy");
@@ -836,15 +897,13 @@ static const mg_options *opts_or_default(const mg_options *o, mg_options *d) {
   return d;
 }
 
-extern "C" {
-
-int mg_bfs_multi(mg_graph *g, const int32_t *srcs, int32_t nsrc, int32_t *depths, mg_stats *stats,
-                 const mg_options *opts) {
-  clear_error();
-  if (!g) return set_error(MG_ERR_ARG, "graph is NULL");
-  if (!depths) return set_error(MG_ERR_ARG, "depths is NULL");
-  mg_options d;
-  const mg_options *o = opts_or_default(opts, &d);
+// One batched BFS with DT depth rows. A uint16 run stops after level
+// kMsDepth16Levels; *depth_overflow then tells the caller to rerun with int32.
+template <typename DT>
+static int bfs_multi_run(mg_graph *g, const int32_t *srcs, int32_t nsrc, int32_t *depths, mg_stats *stats,
+                         const mg_options *o, bool *depth_overflow) {
+  constexpr bool d16 = sizeof(DT) == 2;
+  *depth_overflow = false;
   cudaStream_t s = run_stream(g, o);
   SrcList list;
   int st = multi_prepare(g, srcs, nsrc, o, s, &list, -1);
@@ -870,7 +929,8 @@ int mg_bfs_multi(mg_graph *g, const int32_t *srcs, int32_t nsrc, int32_t *depths
   ga.ctl = g->ws.ctl;
   ga.expand_in = 0;
   ga.gather_dir = NO_GATHER_EDGES;
-  const uint32_t max_iter = (uint32_t)std::min<int64_t>(o->iter_num > 0 ? o->iter_num : 0, g->nodes + 2);
+  const uint32_t max_iter_asked = (uint32_t)std::min<int64_t>(o->iter_num > 0 ? o->iter_num : 0, g->nodes + 2);
+  const uint32_t max_iter = d16 ? std::min(max_iter_asked, kMsDepth16Levels) : max_iter_asked;
   const int dir = o->direction;
   // direction policy and switch factors go to the control block with the sources
   list.dir = (uint32_t)dir;
@@ -878,7 +938,7 @@ int mg_bfs_multi(mg_graph *g, const int32_t *srcs, int32_t nsrc, int32_t *depths
   list.beta = (float)o->beta;
   k_ctl_init<<<1, 32, 0, s>>>(g->ws.ctl, (uint32_t)list.ndistinct, max_iter, (unsigned long long)o->spin_limit,
                               dir == MG_DIR_PULL ? MODE_BITMAP : MODE_QUEUE, ctl_flags(o));
-  k_ms_init<<<1, 64, 0, s>>>(a, list, 1);
+  k_ms_init<<<1, 64, 0, s>>>(a, list, d16 ? 2 : 1);
   count_launch(2);
   if ((st = launch_check("batched bfs init")) != MG_OK) return st;
   const int grid = persistent_grid(g, o, 4);
@@ -887,19 +947,39 @@ int mg_bfs_multi(mg_graph *g, const int32_t *srcs, int32_t nsrc, int32_t *depths
   const int32_t V = g->csr.V;
   const int64_t E = g->edges;
   LevelBody body = [=](cudaStream_t ss, cudaGraphConditionalHandle h, int use_h) {
-    MG_LAUNCH(KID_MS_APPLY, ss, k_ms_apply<<<grid, kNT, 0, ss>>>(a));
+    MG_LAUNCH(KID_MS_APPLY, ss, k_ms_apply<DT><<<grid, kNT, 0, ss>>>(a));
     MG_LAUNCH(KID_CONVERT, ss, k_ms_convert<<<grid, kNT, 0, ss>>>(a));
     MG_LAUNCH(KID_SCAN, ss, (k_frontier_scan<msbfs_push, kMVTS, kMVT><<<grid, kNT, 0, ss>>>(ga)));
     MG_LAUNCH(KID_EXPAND, ss, (k_expand<msbfs_push, kMVT><<<grid, kNT, 0, ss>>>(ga)));
-    MG_LAUNCH(KID_MS_PULL, ss, k_ms_pull<<<pull_grid, kNT, 0, ss>>>(a));
+    MG_LAUNCH(KID_MS_PULL, ss, k_ms_pull<DT><<<pull_grid, kNT, 0, ss>>>(a));
     MG_LAUNCH(KID_OTHER, ss, k_ms_level_end<<<1, 32, 0, ss>>>(a.ctl, V, E, h, use_h));
   };
   LoopResult res;
-  const auto epi = transpose_epilogue(g, nsrc, depths, true);
-  st = run_level_loop(g, s, "bfs_multi/" + std::to_string(grid), 6, body, o->use_cuda_graph != 0, &res,
-                      o->outputs_on_device ? &epi : nullptr);
+  const auto epi = transpose_epilogue(g, nsrc, depths, true, d16);
+  st = run_level_loop(g, s, std::string(d16 ? "bfs_multi16/" : "bfs_multi/") + std::to_string(grid), 6, body,
+                      o->use_cuda_graph != 0, &res, o->outputs_on_device ? &epi : nullptr);
   if (st != MG_OK) return st;
-  return multi_finish(g, s, nsrc, depths, -1, stats, o, res);
+  if (d16 && res.ctl.frontier_size > 0 && res.ctl.level >= kMsDepth16Levels && max_iter_asked > kMsDepth16Levels) {
+    finish_run(g, res.ctl.level);
+    *depth_overflow = true;  // deeper than a uint16 depth row holds
+    return MG_OK;
+  }
+  return multi_finish(g, s, nsrc, depths, -1, stats, o, res, d16);
+}
+
+extern "C" {
+
+int mg_bfs_multi(mg_graph *g, const int32_t *srcs, int32_t nsrc, int32_t *depths, mg_stats *stats,
+                 const mg_options *opts) {
+  clear_error();
+  if (!g) return set_error(MG_ERR_ARG, "graph is NULL");
+  if (!depths) return set_error(MG_ERR_ARG, "depths is NULL");
+  mg_options d;
+  const mg_options *o = opts_or_default(opts, &d);
+  bool overflow = false;
+  int st = bfs_multi_run<uint16_t>(g, srcs, nsrc, depths, stats, o, &overflow);
+  if (st != MG_OK || !overflow) return st;
+  return bfs_multi_run<int32_t>(g, srcs, nsrc, depths, stats, o, &overflow);
 }
 
 int mg_sssp_multi(mg_graph *g, const int32_t *srcs, int32_t nsrc, int32_t *dists, mg_stats *stats,
@@ -947,11 +1027,11 @@ int mg_sssp_multi(mg_graph *g, const int32_t *srcs, int32_t nsrc, int32_t *dists
     MG_LAUNCH(KID_OTHER, ss, k_mss_level_end<<<1, 32, 0, ss>>>(a.ctl, h, use_h));
   };
   LoopResult res;
-  const auto epi = transpose_epilogue(g, nsrc, dists, false);
+  const auto epi = transpose_epilogue(g, nsrc, dists, false, false);
   st = run_level_loop(g, s, "sssp_multi/" + std::to_string(grid), 4, body, o->use_cuda_graph != 0, &res,
                       o->outputs_on_device ? &epi : nullptr);
   if (st != MG_OK) return st;
-  return multi_finish(g, s, nsrc, dists, programs::sssp::INIT_VALUE, stats, o, res);
+  return multi_finish(g, s, nsrc, dists, programs::sssp::INIT_VALUE, stats, o, res, false);
 }
 
 }  // extern "C"

@@ -114,7 +114,7 @@ int64_t mg_kernel_launches(int reset);
  * bracketed by CUDA events; enabling resets the accumulators. */
 int mg_profile_enable(int enable);
 /* Accumulated time, launch count and algorithmic bytes of kernel kind `kind`
- * (0 <= kind < 12); *name receives a static string. */
+ * (0 <= kind < 13); *name receives a static string. */
 int mg_profile_read(int32_t kind, const char **name, double *total_ms, int64_t *launches, uint64_t *bytes);
 /* Failure-detection self-test (no reference counterpart; the reference exits
  * on errors, GASengine/enactor_vertex_centric.cuh:107-129): runs the library's

@@ -7,13 +7,18 @@
 // This header keeps those names, argument meanings and the cudaError_t-style
 // "return a status, do not throw" behaviour, so a driver written against the
 // reference ports by changing includes. The four bundled Programs are tags
-// (mapgraph::bfs, sssp, cc, pagerank); a new device Program drops into the
-// template engine gpugraph_b200/csrc/gas/engine.cuh instead.
+// (mapgraph::bfs, sssp, cc, pagerank) served by the library's specialised
+// kernels. Any other Program -- a struct written in the reference's form, with
+// Initialize, the device functors and extractResult -- runs through the same
+// CsrProblem / EnactorVertexCentric calls once its translation unit (compiled
+// by nvcc) includes mapgraph_b200_gas.cuh, which instantiates the generic GAS
+// engine for it.
 #ifndef MAPGRAPH_B200_HPP
 #define MAPGRAPH_B200_HPP
 
 #include <algorithm>
 #include <cstdint>
+#include <memory>
 #include <string>
 #include <type_traits>
 #include <vector>
@@ -61,6 +66,7 @@ class CsrProblem {
                       const int * /*h_column_offsets*/, int /*num_gpus*/, int directed) {
     mg_graph_destroy(g_);
     g_ = nullptr;
+    program_state_.reset();
     nodes_ = nodes;
     return mg_graph_create(h_row_offsets, h_column_indices, h_edge_values,
                            h_edge_values ? MG_VAL_I32 : MG_VAL_NONE, nodes, edges, directed, &opts_, &g_);
@@ -88,8 +94,15 @@ class CsrProblem {
   std::vector<int> &preds() { return preds_; }
   const mg_stats &stats() const { return stats_; }
   mg_stats &stats() { return stats_; }
+  // State a Program in the reference's form keeps between runs (its VertexType
+  // and EdgeType, whose arrays its Initialize allocates once); owned here, set
+  // by the engine in mapgraph_b200_gas.cuh.
+  std::shared_ptr<void> &program_state() { return program_state_; }
 
  private:
+  // program_state_ is declared first so that it is released last, after the
+  // graph (its release may free device memory the graph's last run used)
+  std::shared_ptr<void> program_state_;
   mg_graph *g_ = nullptr;
   mg_options opts_;
   int nodes_ = 0;
@@ -99,6 +112,16 @@ class CsrProblem {
 };
 
 namespace detail {
+// Runs a Program written in the reference's form through the generic GAS
+// engine. Defined in mapgraph_b200_gas.cuh: a translation unit that enacts such
+// a Program includes that header (the bundled tags below do not need it).
+template <class Program, bool M>
+struct ProgramRunner;
+template <class Program, bool M>
+int run(CsrProblem<Program, M> &p, int num_srcs, const int *srcs) {
+  return ProgramRunner<Program, M>::run(p, num_srcs, srcs);
+}
+
 template <bool M>
 int run(CsrProblem<bfs, M> &p, int num_srcs, const int *srcs) {
   p.result().resize((size_t)p.nodes());

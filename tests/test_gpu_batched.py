@@ -171,3 +171,23 @@ def test_graph_batch_with_trivial_graphs():
     for i, h in enumerate(graphs):
         b, e = big.graph_offsets[i], big.graph_offsets[i + 1]
         assert np.array_equal(out[b:e], oracle.bfs(h.row_offsets, h.column_indices, local[i])), i
+
+
+def test_bfs_multi_deeper_than_16bit_depth_rows():
+    # a path of 66,000 vertices: depths past 65,534 do not fit the 16-bit depth rows
+    # the batched BFS keeps, so the run is redone with 32-bit rows; a shallower
+    # source set on the same graph stays on the 16-bit rows
+    n = 66000
+    ro = np.concatenate([[0], np.cumsum([1] + [2] * (n - 2) + [1])]).astype(np.int32)
+    col = np.empty(ro[-1], np.int32)
+    for v in range(n):
+        nb = [u for u in (v - 1, v + 1) if 0 <= u < n]
+        col[ro[v]:ro[v + 1]] = nb
+    hg = HostGraph(ro, col, None)
+    g = Graph(hg)
+    for srcs in (np.array([0, n - 1, n // 2], np.int32), np.array([n // 2, n // 2 + 7], np.int32)):
+        out, st = g.bfs_multi(srcs, direction=_lib.MG_DIR_PUSH)
+        ref = np.stack([oracle.bfs(ro, col, s) for s in srcs])
+        assert np.array_equal(out, ref)
+        assert st["iterations"] >= int(ref.max())
+    assert int(oracle.bfs(ro, col, 0).max()) == n - 1
