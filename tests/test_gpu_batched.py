@@ -191,3 +191,4 @@ def test_bfs_multi_deeper_than_16bit_depth_rows():
         assert np.array_equal(out, ref)
         assert st["iterations"] >= int(ref.max())
     assert int(oracle.bfs(ro, col, 0).max()) == n - 1
+
