@@ -73,7 +73,7 @@ __global__ void __launch_bounds__(kNT, 6) k_bfs_pull(GasArgs<BfsP> a) {
       search[q] = v < V && !((vis[q] >> lane) & 1u);
       if (!search[q]) end[q] = beg[q];  // nothing to scan
 #pragma unroll
-      for (int k = 0; k < 4; ++k) u[q][k] = beg[q] + k < end[q] ? crow[beg[q] + k] : -1;
+      for (int k = 0; k < 4; ++k) u[q][k] = beg[q] + k < end[q] ? __ldcs(crow + beg[q] + k) : -1;
     }
     bool found[kPullWords];
 #pragma unroll
@@ -94,10 +94,10 @@ __global__ void __launch_bounds__(kNT, 6) k_bfs_pull(GasArgs<BfsP> a) {
         // continue four in-edges per step (independent loads in flight)
         while (e < end[q]) {
           const int c = min(4, end[q] - e);
-          const int u0 = crow[e];
-          const int u1 = c > 1 ? crow[e + 1] : u0;
-          const int u2 = c > 2 ? crow[e + 2] : u0;
-          const int u3 = c > 3 ? crow[e + 3] : u0;
+          const int u0 = __ldcs(crow + e);
+          const int u1 = c > 1 ? __ldcs(crow + e + 1) : u0;
+          const int u2 = c > 2 ? __ldcs(crow + e + 2) : u0;
+          const int u3 = c > 3 ? __ldcs(crow + e + 3) : u0;
           const uint32_t hit = ((__ldg(&cur[u0 >> 5]) >> (u0 & 31)) | (__ldg(&cur[u1 >> 5]) >> (u1 & 31)) |
                                 (__ldg(&cur[u2 >> 5]) >> (u2 & 31)) | (__ldg(&cur[u3 >> 5]) >> (u3 & 31))) &
                                1u;
@@ -199,7 +199,7 @@ __global__ void __launch_bounds__(kNT, 6) k_bfs_push(GasArgs<BfsP> a) {
         my_bytes += el >= 0 ? 8ull : 12ull;  // column + visited probe; a vertex's own item: its offsets + queue entry
         if (el >= 0) {
           const int eid = s_rs[j] + el;
-          if ((unsigned)eid < (unsigned)a.g.E) nbr[r] = col[eid];
+          if ((unsigned)eid < (unsigned)a.g.E) nbr[r] = __ldcs(col + eid);
           else raise_error(ctl, MG_ERR_OVERFLOW);
         }
       }

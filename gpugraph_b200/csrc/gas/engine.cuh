@@ -450,7 +450,7 @@ __global__ void __launch_bounds__(kNT) k_expand(GasArgs<P> a) {
             }
           }
           if ((unsigned)eid < (unsigned)a.g.E) {
-            const int nbr = nbp[eid];
+            const int nbr = __ldcs(nbp + eid);
             const int eidv = (in_edge && a.g.csc_eid) ? a.g.csc_eid[eid] : eid;
             typename P::MiscType misc = typename P::MiscType();
             ee(s_ch[j] != 0, (int)level, v, nbr, eidv, a.vl, a.el, fo, misc);

@@ -285,7 +285,7 @@ __global__ void __launch_bounds__(kNT, 5) k_ms_pull(MultiArgs a) {
       if (pulls) {
         int u[kMsSerial];
 #pragma unroll
-        for (int k = 0; k < kMsSerial; ++k) u[k] = b + k < e ? crow[b + k] : -1;
+        for (int k = 0; k < kMsSerial; ++k) u[k] = b + k < e ? __ldcs(crow + b + k) : -1;
 #pragma unroll
         for (int k = 0; k < kMsSerial; ++k)
           if (u[k] >= 0) acc |= __ldg(&Fc[u[k]]);
@@ -304,7 +304,7 @@ __global__ void __launch_bounds__(kNT, 5) k_ms_pull(MultiArgs a) {
           const int i = c + 32 * k + lane;
           x[k] = 0;
           if (i < lim) {
-            x[k] = __ldg(&Fc[crow[i]]);
+            x[k] = __ldg(&Fc[__ldcs(crow + i)]);
             ++probes;
           }
         }
@@ -659,8 +659,8 @@ __global__ void __launch_bounds__(kNT) k_mss_expand(MultiArgs a, const uint32_t 
         return;
       }
       u = s_v[j];
-      v = col[eid];
-      w = wgt[eid];
+      v = __ldcs(col + eid);
+      w = __ldcs(wgt + eid);
       am = Fc[u];
     };
     // next-level mask and dedup bit of the vertices that improved; the ones

@@ -163,7 +163,7 @@ __global__ void __launch_bounds__(kNT, 6) k_pr_iter(PrArgs a) {
       int u[kPrSerial];
       float x[kPrSerial];
 #pragma unroll
-      for (int k = 0; k < kPrSerial; ++k) u[k] = b + k < e ? a.crow[b + k] : -1;
+      for (int k = 0; k < kPrSerial; ++k) u[k] = b + k < e ? __ldcs(a.crow + b + k) : -1;
 #pragma unroll
       for (int k = 0; k < kPrSerial; ++k) x[k] = u[k] >= 0 ? __ldg(&cold[u[k]]) : 0.f;
 #pragma unroll
@@ -179,7 +179,7 @@ __global__ void __launch_bounds__(kNT, 6) k_pr_iter(PrArgs a) {
 #pragma unroll
         for (int k = 0; k < kPrSub; ++k) {
           const int i = c + 32 * k + lane;
-          u[k] = i < seg_e ? a.crow[i] : -1;
+          u[k] = i < seg_e ? __ldcs(a.crow + i) : -1;
         }
 #pragma unroll
         for (int k = 0; k < kPrSub; ++k) x[k] = u[k] >= 0 ? __ldg(&cold[u[k]]) : 0.f;
@@ -209,13 +209,13 @@ __global__ void __launch_bounds__(kNT, 6) k_pr_iter(PrArgs a) {
       int u[8];
       float x[8];
 #pragma unroll
-      for (int j = 0; j < 8; ++j) u[j] = a.crow[k + 32 * j];
+      for (int j = 0; j < 8; ++j) u[j] = __ldcs(a.crow + k + 32 * j);
 #pragma unroll
       for (int j = 0; j < 8; ++j) x[j] = __ldg(&cold[u[j]]);
 #pragma unroll
       for (int j = 0; j < 8; ++j) acc += x[j];
     }
-    for (; k < ce; k += 32) acc += __ldg(&cold[a.crow[k]]);
+    for (; k < ce; k += 32) acc += __ldg(&cold[__ldcs(a.crow + k)]);
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
     if (lane == 0) {
