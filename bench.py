@@ -231,9 +231,17 @@ def run_native(args, world: int):
     stream = torch.cuda.current_stream()
     graphs = 0 if args.no_cuda_graph else 1
     base_opts = dict(outputs_on_device=1, stream=stream.cuda_stream, compute_stats=0, use_cuda_graph=graphs)
-    o_multi = _lib.default_options(**base_opts)
     st = _lib.Stats()
     src_arr = np.ascontiguousarray(srcs)
+    # launch shape and direction factors from the library's autotuner, on this graph and these
+    # sources (untimed); the default options are timed beside them in sub_results
+    tuned = {}
+    if not args.no_autotune:
+        from gpugraph_b200.autotune import autotune
+
+        tuned, _ = autotune(g, "bfs_multi", src_arr, **base_opts)
+    o_multi = _lib.default_options(**dict(base_opts, **tuned))
+    o_default = _lib.default_options(**base_opts)
 
     def multi_step(opts=o_multi):
         _lib.check(lib.mg_bfs_multi(g.handle, src_arr.ctypes.data, NSRC, out_dev.data_ptr(), None, opts),
@@ -267,11 +275,15 @@ def run_native(args, world: int):
     rate, step_s = replicas.aggregate_rate(teps_edges, ev0.elapsed_time(ev1) / args.steps * 1e-3, str(dev))
     value = rate / 1e9
     sub = {"bfs_batched64": {"gteps_this_rank": teps_edges / (ev0.elapsed_time(ev1) / args.steps * 1e-3) / 1e9,
-                             "ms": step_s * 1e3, "levels": levels_multi, "vertices_reached": reached_total}}
+                             "ms": step_s * 1e3, "levels": levels_multi, "vertices_reached": reached_total,
+                             "autotuned_options": tuned}}
+    if tuned:
+        dms = _time_events(lambda: multi_step(o_default), stream, max(3, min(args.steps, 10)))
+        sub["bfs_batched64"]["default_options_ms"] = dms
 
     # ---- end to end through the C ABI with host buffers (pinned), one call per step
     host_out = torch.empty((NSRC, hg.nodes), dtype=torch.int32, pin_memory=True)
-    o_host = _lib.default_options(stream=stream.cuda_stream, compute_stats=0, use_cuda_graph=graphs)
+    o_host = _lib.default_options(stream=stream.cuda_stream, compute_stats=0, use_cuda_graph=graphs, **tuned)
     src_pinned = torch.from_numpy(src_arr.copy()).pin_memory()
     _lib.check(lib.mg_bfs_multi(g.handle, src_pinned.data_ptr(), NSRC, host_out.data_ptr(), None, o_host), "e2e")
     torch.cuda.synchronize()
@@ -307,7 +319,7 @@ def run_native(args, world: int):
         sub.update(single_gpu_configs(args, hg, g, srcs, out_dev, teps_edges, reached_total, value, stream, peak))
         sub.update(extra_configs(dev, stream, peak))
 
-    res = {"value": value, "ms_per_step": step_s * 1e3, "launches": launches, "sub": sub, "e2e": e2e,
+    res = {"value": value, "ms_per_step": step_s * 1e3, "launches": launches, "sub": sub, "e2e": e2e, "tuned": tuned,
            "roofline": roofline, "clocks": clk.summary(), "V": hg.nodes, "E": hg.edges,
            "teps_edges_this_rank": teps_edges}
     g.close()
@@ -572,6 +584,7 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-cuda-graph", action="store_true",
                     help="launch the same level kernels host-driven (for ncu launch lists)")
+    ap.add_argument("--no-autotune", action="store_true", help="time the headline with the default options")
     args = ap.parse_args()
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -628,7 +641,8 @@ def main():
                 "impl": "native", "metric": metric, "value": res["value"], "unit": "GTEPS", "n_gpus": world,
                 "steps": args.steps, "warmup": args.warmup, "ms_per_step": res["ms_per_step"],
                 "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "int32",
-                "data": "synthetic", "config": config, "e2e": res["e2e"], "roofline": res["roofline"],
+                "data": "synthetic", "config": dict(config, options=res["tuned"] or "defaults"),
+                "e2e": res["e2e"], "roofline": res["roofline"],
                 "cpu_baseline": cpu, "gpu_launches": res["launches"], "clocks": res["clocks"],
                 "sub_results": res["sub"],
                 "graph": {"V": res["V"], "E": res["E"], "teps_edges_rank0": res["teps_edges_this_rank"]},

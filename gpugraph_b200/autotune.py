@@ -16,7 +16,7 @@ import numpy as np
 from . import _lib
 from ._lib import check, default_options, lib
 
-KINDS = {"bfs": 0, "bfs_multi": 1, "sssp": 2, "cc": 3}
+KINDS = {"bfs": 0, "bfs_multi": 1, "sssp": 2, "cc": 3, "pagerank": 4, "ppr": 5}
 TUNED = ("tile_items", "ctas_per_sm", "alpha", "alpha_multi", "beta")
 
 

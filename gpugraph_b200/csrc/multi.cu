@@ -195,6 +195,116 @@ __global__ void __launch_bounds__(kNT) k_ms_apply(MultiArgs a) {
   if (lane_id() == 0 && act) atomicOr(&ctl->srcmask[L & 1], act);
 }
 
+// Push level of the batched BFS, fused (the msbfs_push Program's expand_edge
+// and contract with the engine's dedup and compaction): tiles of NV = kNT*VT
+// items from the frontier scan's merge-path partition; every thread takes its
+// VT items through batches of independent memory operations -- all column
+// loads, then all tail-mask and head-visit loads, then the OR of the new
+// sources into the heads' next masks (reductions, nothing to wait for) with
+// the dedup-bitmap probes, then the test-and-sets -- instead of one dependent
+// chain per item; heads that win their dedup bit are compacted into the next
+// queue with one reservation per tile.
+template <int VT>
+__global__ void __launch_bounds__(kNT, 4) k_ms_push(GasArgs<msbfs_push> a) {
+  constexpr int NV = kNT * VT;
+  __shared__ int32_t s_v[NV + 1];
+  __shared__ int32_t s_base[NV + 1];
+  __shared__ int32_t s_rs[NV + 1];
+  __shared__ int32_t s_own[NV];
+  __shared__ uint32_t s_cnt[VT * kNW + 1];
+  __shared__ uint32_t s_tile, s_prefix;
+  __shared__ int s_fail;
+  __shared__ unsigned long long s_edges;
+  Ctl *ctl = a.ctl;
+  if (!ctl->active || ctl->mode != MODE_QUEUE) return;
+  const uint32_t level = ctl->level, n = ctl->frontier_size, total = ctl->edge_total;
+  const uint32_t ntiles = ctl->exp_tiles, epoch = ctl->epoch + 1;
+  const unsigned long long spin_limit = ctl->spin_limit;
+  const bool ordered = ctl->ordered != 0;
+  const unsigned long long items = (unsigned long long)n + total;
+  const int32_t *F = cur_queue(a, level);
+  int32_t *Fout = nxt_queue(a, level);
+  uint32_t *dedup = nxt_bm(a, level);
+  const u64 *Fc = (level & 1) ? a.vl.F1 : a.vl.F0;
+  u64 *Fn = (level & 1) ? a.vl.F0 : a.vl.F1;
+  const u64 *visit = a.vl.visit;
+  const int32_t *ro = a.g.row_offsets, *col = a.g.col;
+  const int32_t V = a.g.V;
+  const int lane = lane_id();
+  unsigned long long my_edges = 0, my_bytes = 0;
+  if (threadIdx.x == 0) {
+    s_fail = 0;
+    s_edges = 0;
+  }
+  for (;;) {
+    const uint32_t tile = next_tile(&ctl->tile_ctr[1], &s_tile);
+    if (tile >= ntiles || s_fail) break;
+    int cnt;
+    if (!decode_tile<VT>(tile, ntiles, n, items, a.part, a.scan, F, ro, s_v, s_base, s_rs, s_own, &cnt,
+                         [](int, int) {})) {
+      if (threadIdx.x == 0) {
+        raise_error(ctl, MG_ERR_OVERFLOW);
+        s_fail = 1;
+      }
+      __syncthreads();
+      break;
+    }
+    int32_t head[VT], tail[VT];
+#pragma unroll
+    for (int r = 0; r < VT; ++r) {
+      const int k = r * kNT + threadIdx.x;
+      head[r] = -1;
+      tail[r] = 0;
+      if (k < cnt) {
+        const int j = s_own[k];
+        const int el = k - s_base[j] - 1;
+        my_bytes += 12;  // column + head visit mask, or a vertex's own item: offsets + queue entry
+        if (el >= 0) {
+          const int eid = s_rs[j] + el;
+          tail[r] = s_v[j];
+          if ((unsigned)eid < (unsigned)a.g.E) head[r] = __ldcs(col + eid);
+          else raise_error(ctl, MG_ERR_OVERFLOW);
+        }
+      }
+    }
+    u64 m[VT];
+#pragma unroll
+    for (int r = 0; r < VT; ++r) {
+      m[r] = 0;
+      if ((unsigned)head[r] < (unsigned)V) m[r] = __ldg(Fc + tail[r]) & ~__ldg(visit + head[r]);
+    }
+    uint32_t probe[VT];
+#pragma unroll
+    for (int r = 0; r < VT; ++r) {
+      probe[r] = ~0u;
+      if (m[r]) {
+        atomicOr(&Fn[head[r]], m[r]);  // result unused: a reduction
+        probe[r] = ld_volatile(&dedup[head[r] >> 5]);
+        my_bytes += 8;
+      }
+    }
+    uint32_t bal[VT];
+#pragma unroll
+    for (int r = 0; r < VT; ++r) {
+      const uint32_t bit = 1u << (head[r] & 31);
+      const bool surv = m[r] && !(probe[r] & bit) && !(atomicOr(&dedup[head[r] >> 5], bit) & bit);
+      if (surv) {
+        my_edges += (unsigned long long)(ro[head[r] + 1] - ro[head[r]]);
+        my_bytes += 8;  // queue entry + next-mask word
+      }
+      bal[r] = __ballot_sync(0xffffffffu, surv);
+    }
+    if (!tile_enqueue<VT>(bal, head, s_cnt, &s_prefix, &s_fail, ordered, a.status, tile, ntiles, epoch, spin_limit,
+                          Fout, (uint32_t)V, ctl))
+      break;
+  }
+  add_bytes(ctl, KID_EXPAND, my_bytes);
+  my_edges = warp_sum(my_edges);
+  if (lane == 0 && my_edges) atomicAdd(&s_edges, my_edges);
+  __syncthreads();
+  if (threadIdx.x == 0 && s_edges) atomicAdd(&ctl->next_edges, s_edges);
+}
+
 // OR of a 64-bit value over the warp.
 MG_DEVINL u64 warp_or(u64 x) {
 #pragma unroll
@@ -950,7 +1060,7 @@ static int bfs_multi_run(mg_graph *g, const int32_t *srcs, int32_t nsrc, int32_t
     MG_LAUNCH(KID_MS_APPLY, ss, k_ms_apply<DT><<<grid, kNT, 0, ss>>>(a));
     MG_LAUNCH(KID_CONVERT, ss, k_ms_convert<<<grid, kNT, 0, ss>>>(a));
     MG_LAUNCH(KID_SCAN, ss, (k_frontier_scan<msbfs_push, kMVTS, kMVT><<<grid, kNT, 0, ss>>>(ga)));
-    MG_LAUNCH(KID_EXPAND, ss, (k_expand<msbfs_push, kMVT><<<grid, kNT, 0, ss>>>(ga)));
+    MG_LAUNCH(KID_EXPAND, ss, (k_ms_push<kMVT><<<grid, kNT, 0, ss>>>(ga)));
     MG_LAUNCH(KID_MS_PULL, ss, k_ms_pull<DT><<<pull_grid, kNT, 0, ss>>>(a));
     MG_LAUNCH(KID_OTHER, ss, k_ms_level_end<<<1, 32, 0, ss>>>(a.ctl, V, E, h, use_h));
   };

@@ -226,15 +226,20 @@ int mg_bfs_noalloc(const int32_t *d_row_offsets, const int32_t *d_column_indices
                    int64_t edges, int32_t src, int32_t *d_depths, void *stream, mg_stats *stats);
 
 /* ------------------------------------------------------------- autotuner -- */
-enum { MG_TUNE_BFS = 0, MG_TUNE_BFS_MULTI = 1, MG_TUNE_SSSP = 2, MG_TUNE_CC = 3 };
+enum { MG_TUNE_BFS = 0, MG_TUNE_BFS_MULTI = 1, MG_TUNE_SSSP = 2, MG_TUNE_CC = 3, MG_TUNE_PAGERANK = 4,
+       MG_TUNE_PPR = 5 };
 /* Chooses the launch parameters the reference fixes at compile time
  * (KernelPolicy and the CTA/warp gather thresholds,
  * GASengine/enactor_vertex_centric.cuh:3934-3970) by timing candidates on this
  * graph and these sources: expand tile (tile_items 1024/2048) x ctas_per_sm
  * (2..5), then alpha (or alpha_multi) and beta for the direction switch.
+ * MG_TUNE_PAGERANK (mg_pagerank) and MG_TUNE_PPR (mg_ppr_forward) search
+ * ctas_per_sm of their SpMV (2..8), timing a fixed number of iterations; PPR
+ * solves nsrc teleport columns, one-hot at srcs, over row-normalised uniform
+ * weights (the launch shape does not depend on the values).
  * *inout is the starting point and receives the best options; report (may be
  * NULL) receives a JSON record of every trial. srcs: 1..64 sources (unused for
- * MG_TUNE_CC). */
+ * MG_TUNE_CC and MG_TUNE_PAGERANK). */
 int mg_autotune(mg_graph *g, int32_t kind, const int32_t *srcs, int32_t nsrc, mg_options *inout,
                 char *report, int64_t report_len);
 

@@ -30,3 +30,30 @@ def test_autotune_bfs_multi_and_sssp(tmp_path):
     assert np.array_equal(d, oracle.sssp(hg.row_offsets, hg.column_indices, hg.edge_values, srcs[0]))
     best_b, _ = autotune(g, "bfs", srcs[:4])
     assert np.array_equal(g.bfs(int(srcs[1]), **best_b)[0], oracle.bfs(hg.row_offsets, hg.column_indices, srcs[1]))
+
+
+def test_autotune_pagerank_and_ppr():
+    import torch
+
+    from gpugraph_b200.ppr import ppr
+
+    hg = HostGraph.rmat(13, 8, seed=5, symmetrize=False)
+    g = Graph(hg, directed=True)
+    best, report = autotune(g, "pagerank")
+    assert 2 <= best["ctas_per_sm"] <= 8 and len(report["trials"]) == 7
+    t = hg.transpose()
+    r, st = g.pagerank(ctas_per_sm=best["ctas_per_sm"])
+    ref, _, _ = oracle.pagerank_fp64(hg.row_offsets, t.row_offsets, t.column_indices, 0.85, 0.0, st["iterations"])
+    assert np.abs(r - ref).sum() <= 1e-6
+    srcs = np.array([0, 5, 77, 4000], np.int32)
+    best_p, report_p = autotune(g, "ppr", srcs)
+    assert 2 <= best_p["ctas_per_sm"] <= 8 and len(report_p["trials"]) == 7
+    src = np.repeat(np.arange(hg.nodes), np.diff(hg.row_offsets))
+    w = 1.0 / np.diff(hg.row_offsets)[src]
+    T = np.zeros((hg.nodes, 4), np.float32)
+    T[srcs, np.arange(4)] = 1.0
+    wt = torch.tensor(w, dtype=torch.float32, device="cuda")
+    Tt = torch.tensor(T, device="cuda")
+    a = ppr(g, wt, Tt)
+    b = ppr(g, wt, Tt, ctas_per_sm=best_p["ctas_per_sm"])
+    assert torch.allclose(a, b, atol=1e-6)
