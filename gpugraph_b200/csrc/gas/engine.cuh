@@ -425,13 +425,16 @@ __global__ void __launch_bounds__(kNT) k_expand(GasArgs<P> a) {
       break;
     }
     __syncthreads();
-    uint32_t bal[VT];
-    int32_t outv[VT];
+    // The thread's VT items go through the Program in phases, so the memory
+    // operations of one phase are independent and in flight together: the
+    // neighbour ids, then every expand_edge, then every contract (as the
+    // reference engine runs expand over the whole edge frontier before
+    // contract), then the dedup probes, then the test-and-sets.
+    int nbr[VT], vv[VT], eidv[VT], jj[VT];
 #pragma unroll
     for (int r = 0; r < VT; ++r) {
       const int k = r * kNT + threadIdx.x;
-      bool surv = false;
-      int fo = -1;
+      nbr[r] = -1;
       if (k < cnt) {
         const int j = s_own[k];
         const int el = k - s_base[j] - 1;
@@ -450,35 +453,58 @@ __global__ void __launch_bounds__(kNT) k_expand(GasArgs<P> a) {
             }
           }
           if ((unsigned)eid < (unsigned)a.g.E) {
-            const int nbr = __ldcs(nbp + eid);
-            const int eidv = (in_edge && a.g.csc_eid) ? a.g.csc_eid[eid] : eid;
-            typename P::MiscType misc = typename P::MiscType();
-            ee(s_ch[j] != 0, (int)level, v, nbr, eidv, a.vl, a.el, fo, misc);
-            if (fo >= V) {
-              raise_error(ctl, MG_ERR_OVERFLOW);
-              fo = -1;
-            }
-            if (fo >= 0) ct((int)level, fo, a.vl, a.el, a.gather_tmp, misc);
-            if (fo >= V) {
-              raise_error(ctl, MG_ERR_OVERFLOW);
-              fo = -1;
-            }
+            nbr[r] = __ldcs(nbp + eid);
+            vv[r] = v;
+            jj[r] = j;
+            eidv[r] = (in_edge && a.g.csc_eid) ? a.g.csc_eid[eid] : eid;
           } else {
             raise_error(ctl, MG_ERR_OVERFLOW);
           }
-          if (fo >= 0) {
-            const uint32_t bit = 1u << (fo & 31);
-            uint32_t *w = dedup + (fo >> 5);
-            if (!(ld_volatile(w) & bit)) surv = !(atomicOr(w, bit) & bit);
-          }
-          if (track_next_edges_trait<P>::value && surv) {
-            my_edges += (unsigned long long)(ro[fo + 1] - ro[fo]);
-            if (both) my_edges += (unsigned long long)(a.g.csc_offsets[fo + 1] - a.g.csc_offsets[fo]);
-          }
         }
       }
+    }
+    int fo[VT];
+    typename P::MiscType misc[VT];
+#pragma unroll
+    for (int r = 0; r < VT; ++r) {
+      fo[r] = -1;
+      misc[r] = typename P::MiscType();
+      if (nbr[r] >= 0) {
+        ee(s_ch[jj[r]] != 0, (int)level, vv[r], nbr[r], eidv[r], a.vl, a.el, fo[r], misc[r]);
+        if (fo[r] >= V) {
+          raise_error(ctl, MG_ERR_OVERFLOW);
+          fo[r] = -1;
+        }
+      }
+    }
+#pragma unroll
+    for (int r = 0; r < VT; ++r) {
+      if (fo[r] >= 0) {
+        ct((int)level, fo[r], a.vl, a.el, a.gather_tmp, misc[r]);
+        if (fo[r] >= V) {
+          raise_error(ctl, MG_ERR_OVERFLOW);
+          fo[r] = -1;
+        }
+      }
+    }
+    uint32_t probe[VT];
+#pragma unroll
+    for (int r = 0; r < VT; ++r) probe[r] = fo[r] >= 0 ? ld_volatile(dedup + (fo[r] >> 5)) : ~0u;
+    uint32_t bal[VT];
+    int32_t outv[VT];
+#pragma unroll
+    for (int r = 0; r < VT; ++r) {
+      bool surv = false;
+      if (fo[r] >= 0) {
+        const uint32_t bit = 1u << (fo[r] & 31);
+        if (!(probe[r] & bit)) surv = !(atomicOr(dedup + (fo[r] >> 5), bit) & bit);
+      }
+      if (track_next_edges_trait<P>::value && surv) {
+        my_edges += (unsigned long long)(ro[fo[r] + 1] - ro[fo[r]]);
+        if (both) my_edges += (unsigned long long)(a.g.csc_offsets[fo[r] + 1] - a.g.csc_offsets[fo[r]]);
+      }
       bal[r] = __ballot_sync(0xffffffffu, surv);
-      outv[r] = fo;
+      outv[r] = fo[r];
       if (surv) my_bytes += 8;  // queue entry + the Program's per-vertex write
     }
     if (!tile_enqueue<VT>(bal, outv, s_cnt, &s_prefix, &s_fail, ordered, a.status, tile, ntiles, epoch, spin_limit,

@@ -577,13 +577,12 @@ __global__ void k_ms_level_end(Ctl *ctl, int32_t V, int64_t E, cudaGraphConditio
 // whose visit bit is clear is unreached: it comes out as -1, and its slot,
 // which the traversal never wrote, is not read (a 16-byte piece with no bits
 // set is not read at all).
-constexpr int kTrV = 64;
-
 template <typename T>
 struct TrShape {
-  static constexpr int kPer = 16 / (int)sizeof(T);  // entries per 16-byte piece
-  static constexpr int kPieces = 64 / kPer;         // pieces per row
-  static constexpr int kQ = kTrV * kPieces / 256;   // pieces per thread per tile
+  static constexpr int kV = sizeof(T) == 2 ? 128 : 64;  // vertices per tile (4 KB of each row type in flight)
+  static constexpr int kPer = 16 / (int)sizeof(T);     // entries per 16-byte piece
+  static constexpr int kPieces = 64 / kPer;            // pieces per row
+  static constexpr int kQ = kV * kPieces / 256;        // pieces per thread per tile
 };
 
 template <typename T>
@@ -613,7 +612,7 @@ MG_DEVINL int32_t tr_entry(const int4 &q, int i) {
 template <typename T>
 __global__ void __launch_bounds__(256, 6) k_ms_transpose(const T *in, const u64 *visit, int32_t *out, int32_t V,
                                                       int32_t s_begin, int32_t ns) {
-  constexpr int PER = TrShape<T>::kPer, PIECES = TrShape<T>::kPieces, Q = TrShape<T>::kQ;
+  constexpr int PER = TrShape<T>::kPer, PIECES = TrShape<T>::kPieces, Q = TrShape<T>::kQ, kTrV = TrShape<T>::kV;
   __shared__ int32_t t[kTrV][65];
   const int64_t ntiles = ((int64_t)V + kTrV - 1) / kTrV;
   const int lane = lane_id(), warp = warp_id();
@@ -644,7 +643,8 @@ __global__ void __launch_bounds__(256, 6) k_ms_transpose(const T *in, const u64 
 static void launch_transpose(mg_graph *g, bool depth16, const u64 *visit, int32_t *out, int32_t nsrc,
                              cudaStream_t s) {
   const int32_t V = g->csr.V;
-  const unsigned nblk = (unsigned)std::min<int64_t>((int64_t)g->num_sms * 6, ((int64_t)V + kTrV - 1) / kTrV);  // 6 CTAs fit on an SM
+  const int kv = depth16 ? TrShape<uint16_t>::kV : TrShape<int32_t>::kV;
+  const unsigned nblk = (unsigned)std::min<int64_t>((int64_t)g->num_sms * 6, ((int64_t)V + kv - 1) / kv);  // 6 CTAs fit on an SM
   if (depth16)
     k_ms_transpose<uint16_t><<<nblk, 256, 0, s>>>(reinterpret_cast<const uint16_t *>(g->multi_out), visit, out, V, 0,
                                                   nsrc);
