@@ -112,21 +112,30 @@ __global__ void __launch_bounds__(kNT, 5) k_sssp_relax(GasArgs<sssp_relax> a) {
     int32_t dv[VT];
 #pragma unroll
     for (int r = 0; r < VT; ++r) dv[r] = ((unsigned)head[r] < (unsigned)V) ? __ldcg(&dist[head[r]]) : INT_MIN;
+    // An improving candidate lowers the distance with a reduction (nothing waits
+    // for the old value); its improvement is read from the loaded distance. If
+    // another relaxation lowered the head further in between, the head is queued
+    // by that relaxation too, so the next frontier is the same set.
     bool better[VT];
+    uint32_t probe[VT];
 #pragma unroll
-    for (int r = 0; r < VT; ++r)
-      better[r] = head[r] >= 0 && cand[r] < dv[r] && atomicMin(&dist[head[r]], cand[r]) > cand[r];
+    for (int r = 0; r < VT; ++r) {
+      better[r] = head[r] >= 0 && cand[r] < dv[r];
+      probe[r] = ~0u;
+      if (better[r]) {
+        atomicMin(&dist[head[r]], cand[r]);
+        probe[r] = ld_volatile(dedup + (head[r] >> 5));
+        my_bytes += 4;  // the improved distance
+      }
+    }
     uint32_t bal[VT];
     int32_t outv[VT];
 #pragma unroll
     for (int r = 0; r < VT; ++r) {
       bool surv = false;
       if (better[r]) {
-        const int u = head[r];
-        const uint32_t bit = 1u << (u & 31);
-        uint32_t *w = dedup + (u >> 5);
-        if (!(ld_volatile(w) & bit)) surv = !(atomicOr(w, bit) & bit);
-        my_bytes += 4;  // the improved distance
+        const uint32_t bit = 1u << (head[r] & 31);
+        if (!(probe[r] & bit)) surv = !(atomicOr(dedup + (head[r] >> 5), bit) & bit);
       }
       if (surv) my_bytes += 8;  // queue entry + dedup word
       bal[r] = __ballot_sync(0xffffffffu, surv);
