@@ -43,6 +43,15 @@ struct Ctl {
   uint32_t prev_size;       // |F| of the previous level (batched traversals)
   uint32_t apply_pending;   // 1: the previous push level left bits to apply
   uint32_t count_bytes;     // 1: kernels add their algorithmic bytes to kbytes (profiling)
+  // Batched BFS level stack: the frontier masks of levels below stk_levels are
+  // kept, one [V] array per level (bit L of stk_pull: level L's array was written
+  // for every vertex by a pull level; otherwise only the queued vertices' entries
+  // are valid, marked in that level's bitmap). clear_pending: the previous
+  // level's parity masks are cleared at its queue entries before this level's
+  // push writes into them.
+  uint32_t stk_levels;
+  uint32_t stk_pull;
+  uint32_t clear_pending;
   // Batched BFS: OR of the frontier masks of level parity p (the sources that
   // can still reach new vertices); accumulated while the level's masks are
   // produced, cleared once consumed.

@@ -87,6 +87,9 @@ int ensure_multi(mg_graph *g) {
     if ((st = device_alloc(g, (void **)&g->multi_out, V * 64 * 4)) != MG_OK) return st;
     g->multi_bytes = V * 64 * 4;
   }
+  if (!g->multi_stk_bm &&
+      (st = device_alloc(g, (void **)&g->multi_stk_bm, (size_t)kMsStackLevels * ((V + 31) / 32) * 4)) != MG_OK)
+    return st;
   return MG_OK;
 }
 

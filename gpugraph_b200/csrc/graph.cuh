@@ -26,6 +26,11 @@
 
 namespace mg {
 
+// Levels of a batched BFS whose frontier masks are kept (the level stack); the
+// [V][64] result buffer holds them ([16][V] u64 = 128 bytes per vertex) beside
+// the uint16 depth rows (another 128 bytes per vertex).
+constexpr uint32_t kMsStackLevels = 16;
+
 struct DevCsr {
   int32_t *row_offsets = nullptr;
   int32_t *col = nullptr;
@@ -89,7 +94,11 @@ struct mg_graph {
   int32_t *ref_outdeg = nullptr;        // reference PageRank out-degree (PageRank.h:141-161)
   // Batched (mask-frontier) working set, allocated on first use.
   unsigned long long *mask[3] = {nullptr, nullptr, nullptr};
-  int32_t *multi_out = nullptr;         // [V][64] int32 per-source results
+  // [V][64] int32 per-source results. A batched BFS with 16-bit depths splits
+  // it: the first half holds the level stack ([kMsStackLevels][V] u64 frontier
+  // masks), the second the [V][64] uint16 depth rows of deeper levels.
+  int32_t *multi_out = nullptr;
+  uint32_t *multi_stk_bm = nullptr;     // [kMsStackLevels][V/32] valid entries of push-made stack levels
   int32_t *multi_stage = nullptr;       // [64][V] transposed results on their way to host memory
   size_t multi_bytes = 0;
   // PageRank plan (built on first mg_pagerank): heavy in-lists split into

@@ -8,12 +8,22 @@
 // HBM layout (per graph, allocated on first use):
 //   mask[0]      visit[V]   u64: bit s set once source s has reached v (BFS)
 //   mask[1..2]   F[2][V]    u64: level-parity frontier masks
-//   multi_out    [V][64]    per-source results: uint16 BFS depths (128 contiguous
-//                           bytes per vertex), or int32 SSSP distances (256 bytes)
-// Results are transposed to the caller's int32 [nsrc][V] layout at the end. A
-// batched BFS keeps 16-bit depths, which halves the bytes of the scattered
-// depth writes and of the transpose's reads; a run that would pass level
-// 65534 stops there and is rerun with int32 depth rows.
+//   multi_out    [V][64]    per-source results: int32 SSSP distances (256 bytes
+//                           per vertex); a batched BFS splits it into the level
+//                           stack and 16-bit depth rows (below)
+// Results are transposed to the caller's int32 [nsrc][V] layout at the end.
+//
+// Batched BFS depths. The frontier masks of levels 0..15 are kept, one [V] u64
+// array per level (the level stack, first half of multi_out): a pull level
+// writes its next masks there for every vertex (a coalesced 32 MB stream at
+// R-MAT scale 22, which the level writes anyway) instead of scattering 2-byte
+// depths into per-vertex rows, and the end-of-run transpose reads the depth of
+// (v, s) as the level whose mask holds bit s. A push level's next masks are
+// ORed into the parity arrays (they need a zeroed target) and copied to the
+// stack for the queued vertices only, with a per-level bitmap of the valid
+// entries. Depths of levels 16 and deeper go to [V][64] uint16 rows (the second
+// half of multi_out); a run that would pass level 65534 stops there and is rerun
+// with int32 depth rows (all of multi_out, no stack).
 //
 // BFS levels switch between push (the GAS engine's load-balanced expand with
 // an OR-into-mask Program, next frontier as a vertex queue) and pull (every
@@ -61,6 +71,7 @@ struct msbfs_push {
     u64 *visit;
     u64 *F0;
     u64 *F1;
+    const u64 *stk;  // level stack ([kMsStackLevels][V]), or null
   };
   struct EdgeType {
     int nodes;
@@ -95,7 +106,11 @@ struct msbfs_push {
 struct MultiArgs {
   DevCsr g;
   u64 *visit, *F0, *F1;
-  int32_t *out;  // [V][64]: int32 rows, or uint16 rows (batched BFS; see depth_rows)
+  int32_t *out;       // [V][64] int32 rows (SSSP)
+  void *rows;         // depth rows of a batched BFS: int32, or uint16 after the level stack
+  u64 *stk;           // level stack [kMsStackLevels][V], or null
+  uint32_t *stk_bm;   // [kMsStackLevels][stk_words] valid entries of push-made stack levels
+  uint32_t stk_words;
   int32_t *q0, *q1;
   uint32_t *bm0, *bm1;
   unsigned long long *status;
@@ -104,9 +119,18 @@ struct MultiArgs {
 };
 
 MG_DEVINL u64 *cur_F(const MultiArgs &a, uint32_t L) { return (L & 1) ? a.F1 : a.F0; }
-// The [V][64] result rows seen as DT (uint16_t or int32_t depths).
+// The [V][64] depth rows seen as DT (uint16_t or int32_t depths).
 template <typename DT>
-MG_DEVINL DT *depth_rows(const MultiArgs &a) { return reinterpret_cast<DT *>(a.out); }
+MG_DEVINL DT *depth_rows(const MultiArgs &a) { return reinterpret_cast<DT *>(a.rows); }
+// Level L's array of the level stack.
+MG_DEVINL u64 *stk_level(const MultiArgs &a, uint32_t L) { return a.stk + (size_t)L * (uint32_t)a.g.V; }
+// The frontier masks of level L: the stack array when a pull level wrote it
+// for every vertex, otherwise the parity array (levels made by a push, whose
+// parity entries are exact, or levels past the stack).
+MG_DEVINL const u64 *front_masks(const MultiArgs &a, const Ctl *ctl, uint32_t L) {
+  if (L < ctl->stk_levels && ((ctl->stk_pull >> L) & 1u)) return stk_level(a, L);
+  return cur_F(a, L);
+}
 // Levels a uint16 depth row can hold (depth 65535 is never written).
 constexpr uint32_t kMsDepth16Levels = 65534;
 MG_DEVINL u64 *nxt_F(const MultiArgs &a, uint32_t L) { return (L & 1) ? a.F0 : a.F1; }
@@ -125,40 +149,62 @@ struct SrcList {
 };
 
 // Level-0 state of a batched run (one CTA of 64 threads).
-// bfs: 0 = SSSP (int32 rows), 1 = BFS with int32 depth rows, 2 = BFS with uint16 rows.
+// bfs: 0 = SSSP (int32 rows), 1 = BFS with int32 depth rows, 2 = BFS with the
+// level stack and uint16 rows.
 __global__ void k_ms_init(MultiArgs a, SrcList L, int bfs) {
   const int t = threadIdx.x;
   if (t < L.nsrc) {
     const int v = L.src[t];
     atomicOr(&a.F0[v], 1ull << t);
     if (bfs) atomicOr(&a.visit[v], 1ull << t);
-    if (bfs == 2) depth_rows<uint16_t>(a)[(int64_t)v * 64 + t] = 0;
-    else a.out[(int64_t)v * 64 + t] = 0;
+    if (bfs == 0) a.out[(int64_t)v * 64 + t] = 0;
+    else if (bfs == 1) depth_rows<int32_t>(a)[(int64_t)v * 64 + t] = 0;
   }
-  if (t < L.ndistinct) a.q0[t] = L.distinct[t];
+  if (t < L.ndistinct) {
+    const int v = L.distinct[t];
+    a.q0[t] = v;
+    if (bfs == 2) {  // level 0 of the stack: each distinct source vertex with its sources
+      u64 m = 0;
+      for (int s = 0; s < L.nsrc; ++s)
+        if (L.src[s] == v) m |= 1ull << s;
+      stk_level(a, 0)[v] = m;
+      atomicOr(&a.stk_bm[v >> 5], 1u << (v & 31));
+    }
+  }
   if (t == 0 && bfs) {
     a.ctl->srcmask[0] = a.all;
     a.ctl->srcmask[1] = 0;
     a.ctl->dir_policy = L.dir;
     a.ctl->alpha = L.alpha;
     a.ctl->beta = L.beta;
+    a.ctl->stk_levels = bfs == 2 ? kMsStackLevels : 0u;
+    a.ctl->stk_pull = 0;
+    a.ctl->clear_pending = 0;
   }
 }
 
-// Start of a level after a push level: the queued vertices keep only their
-// new sources (depth = level), and the previous level's masks are cleared.
+// Start of a level. After a push level (apply_pending) the queued vertices
+// keep only their new sources (depth = level), recorded in the level stack
+// (mask and valid bit) or, past it, in the depth rows. When the previous
+// level's frontier came from a push (clear_pending), its parity masks are
+// cleared at its queue entries, so the parity array is all zero again before
+// this level's push ORs into it.
 template <typename DT>
 __global__ void __launch_bounds__(kNT) k_ms_apply(MultiArgs a) {
   Ctl *ctl = a.ctl;
-  if (!ctl->active || !ctl->apply_pending) return;
-  const uint32_t L = ctl->level, n = ctl->frontier_size, pn = ctl->prev_size;
+  if (!ctl->active || !(ctl->apply_pending | ctl->clear_pending)) return;
+  const uint32_t L = ctl->level, pn = ctl->prev_size;
+  const uint32_t n = ctl->apply_pending ? ctl->frontier_size : 0u;
+  const bool to_stk = L < ctl->stk_levels;
   u64 *Fc = cur_F(a, L), *Fp = nxt_F(a, L);
   const int32_t *Q = cur_Q(a, L), *Qp = nxt_Q(a, L);
+  u64 *Sk = to_stk ? stk_level(a, L) : nullptr;
+  uint32_t *Sb = to_stk ? a.stk_bm + (size_t)L * a.stk_words : nullptr;
   u64 act = 0;
   unsigned long long my_bytes = 0;
   const int lane = lane_id();
-  // whole warps walk the queue, so each new vertex's depths can be written by
-  // the warp together (lane l: sources l and l+32 of the 256-byte row)
+  // whole warps walk the queue, so each new vertex's depth row can be written
+  // by the warp together (lane l: sources l and l+32)
   const uint32_t n_pad = (n + 31) & ~31u;
   for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n_pad; i += gridDim.x * blockDim.x) {
     int v = -1;
@@ -172,9 +218,14 @@ __global__ void __launch_bounds__(kNT) k_ms_apply(MultiArgs a) {
       my_bytes += 28;  // queue entry, visit and mask read, mask write
       if (nb) {
         a.visit[v] = vis | nb;
-        my_bytes += 8 + sizeof(DT) * (unsigned long long)__popcll(nb);
+        my_bytes += 8 + (to_stk ? 12ull : sizeof(DT) * (unsigned long long)__popcll(nb));
+      }
+      if (to_stk) {
+        Sk[v] = nb;
+        atomicOr(&Sb[v >> 5], 1u << (v & 31));
       }
     }
+    if (to_stk) continue;
     uint32_t wv = __ballot_sync(0xffffffffu, nb != 0);
     while (wv) {
       const int j = __ffs(wv) - 1;
@@ -185,9 +236,11 @@ __global__ void __launch_bounds__(kNT) k_ms_apply(MultiArgs a) {
       if ((m >> (lane + 32)) & 1ull) row[lane + 32] = (DT)L;
     }
   }
-  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < pn; i += gridDim.x * blockDim.x) {
-    Fp[Qp[i]] = 0;
-    my_bytes += 12;
+  if (ctl->clear_pending) {
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < pn; i += gridDim.x * blockDim.x) {
+      Fp[Qp[i]] = 0;
+      my_bytes += 12;
+    }
   }
   add_bytes(ctl, KID_MS_APPLY, my_bytes);
 #pragma unroll
@@ -225,11 +278,13 @@ __global__ void __launch_bounds__(kNT, 4) k_ms_push(GasArgs<msbfs_push> a) {
   const int32_t *F = cur_queue(a, level);
   int32_t *Fout = nxt_queue(a, level);
   uint32_t *dedup = nxt_bm(a, level);
-  const u64 *Fc = (level & 1) ? a.vl.F1 : a.vl.F0;
+  const int32_t V = a.g.V;
+  // the tails' masks: the stack array of a level a pull wrote, else the parity array
+  const u64 *Fc = (level < ctl->stk_levels && ((ctl->stk_pull >> level) & 1u)) ? a.vl.stk + (size_t)level * (uint32_t)V
+                                                                               : ((level & 1) ? a.vl.F1 : a.vl.F0);
   u64 *Fn = (level & 1) ? a.vl.F0 : a.vl.F1;
   const u64 *visit = a.vl.visit;
   const int32_t *ro = a.g.row_offsets, *col = a.g.col;
-  const int32_t V = a.g.V;
   const int lane = lane_id();
   unsigned long long my_edges = 0, my_bytes = 0;
   if (threadIdx.x == 0) {
@@ -364,8 +419,12 @@ __global__ void __launch_bounds__(kNT, 5) k_ms_pull(MultiArgs a) {
   if (!ctl->active || ctl->mode != MODE_BITMAP) return;
   const uint32_t L = ctl->level;
   const u64 active_src = ctl->srcmask[L & 1] & a.all;
-  const u64 *Fc = cur_F(a, L);
-  u64 *Fn = nxt_F(a, L);
+  const u64 *Fc = front_masks(a, ctl, L);
+  // next masks: written for every vertex, into the level stack while it has
+  // room (the depths are read from it at the end), else into the parity array
+  // with the new depths written to the rows
+  const bool to_stk = L + 1 < ctl->stk_levels;
+  u64 *Fn = to_stk ? stk_level(a, L + 1) : nxt_F(a, L);
   const int32_t V = a.g.V;
   const int32_t *coff = a.g.csc_offsets, *crow = a.g.pull_rows, *ro = a.g.row_offsets;
   const int lane = lane_id();
@@ -432,12 +491,13 @@ __global__ void __launch_bounds__(kNT, 5) k_ms_pull(MultiArgs a) {
     acc &= need;
     if (valid) Fn[v] = acc;
     if (acc) {
-      my_bytes += 8 + sizeof(DT) * (unsigned long long)__popcll(acc);  // visit write + depths
+      my_bytes += 8 + (to_stk ? 0ull : sizeof(DT) * (unsigned long long)__popcll(acc));  // visit write (+ depths)
       a.visit[v] = vis | acc;
       my_cnt += 1;
       my_edges += (unsigned long long)(ro[v + 1] - ro[v]);
       act |= acc;
     }
+    if (to_stk) continue;
     uint32_t wv = __ballot_sync(0xffffffffu, acc != 0);
     while (wv) {
       const int j = __ffs(wv) - 1;
@@ -463,7 +523,10 @@ __global__ void __launch_bounds__(kNT, 5) k_ms_pull(MultiArgs a) {
 }
 
 // Pull -> push: ordered compaction of the vertices with a non-empty mask into
-// the queue; clears the other parity's masks and both dedup bitmaps.
+// the queue; clears both dedup bitmaps and, when the previous level's masks
+// went to the parity array for every vertex (past the level stack), that array,
+// which the push writes into next. Within the stack the parity arrays are
+// already zero: push-made entries are cleared after use (k_ms_apply).
 __global__ void __launch_bounds__(kNT) k_ms_convert(MultiArgs a) {
   constexpr int VPT = 4;
   constexpr uint32_t TV = kNT * VPT;
@@ -474,8 +537,8 @@ __global__ void __launch_bounds__(kNT) k_ms_convert(MultiArgs a) {
   if (!ctl->active || !ctl->convert) return;
   const uint32_t L = ctl->level, epoch = ctl->epoch + 2;
   const uint32_t V = (uint32_t)a.g.V;
-  const u64 *Fc = cur_F(a, L);
-  u64 *Fo = nxt_F(a, L);
+  const u64 *Fc = front_masks(a, ctl, L);
+  u64 *Fo = (L - 1 >= ctl->stk_levels) ? nxt_F(a, L) : nullptr;
   int32_t *Q = cur_Q(a, L);
   const uint32_t words = (V + 31) / 32;
   for (uint32_t w = blockIdx.x * blockDim.x + threadIdx.x; w < words; w += gridDim.x * blockDim.x) {
@@ -496,7 +559,7 @@ __global__ void __launch_bounds__(kNT) k_ms_convert(MultiArgs a) {
           flags |= 1u << k;
           ++c;
         }
-        Fo[vb + k] = 0;
+        if (Fo) Fo[vb + k] = 0;
       }
     }
     uint32_t tot;
@@ -552,6 +615,10 @@ __global__ void k_ms_level_end(Ctl *ctl, int32_t V, int64_t E, cudaGraphConditio
       if ((double)n_next < (double)V / (double)ctl->beta && n_next < ctl->frontier_size) new_mode = MODE_QUEUE;
     }
     ctl->srcmask[ctl->level & 1] = 0;  // consumed; the level after next accumulates it afresh
+    // this level's parity masks, when a push (or the sources, at level 0) made
+    // them, are cleared at its queue entries at the start of the next level
+    ctl->clear_pending = (mode == MODE_QUEUE || ctl->apply_pending || ctl->level == 0) ? 1u : 0u;
+    if (mode == MODE_BITMAP && ctl->level + 1 < ctl->stk_levels) ctl->stk_pull |= 1u << (ctl->level + 1);
     ctl->apply_pending = (mode == MODE_QUEUE) ? 1u : 0u;
     ctl->convert = (mode == MODE_BITMAP && new_mode == MODE_QUEUE) ? 1u : 0u;
     ctl->mode = new_mode;
@@ -638,16 +705,105 @@ __global__ void __launch_bounds__(256, 6) k_ms_transpose(const T *in, const u64 
   }
 }
 
-// Transposes a run's [V][64] rows (uint16 depths when depth16, else int32) to
-// the caller's [nsrc][V] int32 layout on stream s.
-static void launch_transpose(mg_graph *g, bool depth16, const u64 *visit, int32_t *out, int32_t nsrc,
-                             cudaStream_t s) {
+// Batched BFS depths from the level stack to the caller's int32 [ns][V]
+// layout: the depth of (v, s) is the level L whose stack mask at v holds bit s
+// (a level a pull wrote is valid for every vertex; a push-made level only where
+// its bitmap says so), else, for levels past the stack, the uint16 depth row;
+// -1 where the visit mask lacks bit s. The stack's extent comes from the
+// control block, so the kernel can run as the level loop's epilogue.
+// A warp takes 32 consecutive vertices, one per lane: it loads the valid-entry
+// words and then the masks of up to eight levels at once, folds them into
+// four bit planes of the depth (bit b of plane b set for source s when bit b of
+// its level is set) and the found mask, and then writes the group's entries
+// source by source as 128-byte coalesced stores, each entry taken from the
+// planes with constant shifts. The depth rows are read only by lanes whose
+// vertex has sources reached past the stack.
+constexpr int kTsBatch = 8;  // stack levels whose loads are in flight together
+static_assert(kMsStackLevels == 2 * kTsBatch, "two load batches cover the stack");
+
+template <int B>
+MG_DEVINL void ts_fold(const u64 *stk, const uint32_t *stk_bm, uint32_t words, uint32_t nst, uint32_t full, int32_t V,
+                       uint32_t grp, int64_t v, bool in, int lane, u64 (&p)[4], u64 &found) {
+  uint32_t bw[kTsBatch];
+#pragma unroll
+  for (int k = 0; k < kTsBatch; ++k) {
+    const uint32_t L = B * kTsBatch + k;
+    bw[k] = 0;
+    if (L < nst) bw[k] = ((full >> L) & 1u) ? ~0u : __ldg(&stk_bm[(size_t)L * words + grp]);
+  }
+  u64 m[kTsBatch];
+#pragma unroll
+  for (int k = 0; k < kTsBatch; ++k) {
+    const uint32_t L = B * kTsBatch + k;
+    m[k] = (in && ((bw[k] >> lane) & 1u)) ? __ldcs(&stk[(size_t)L * (uint32_t)V + v]) : 0ull;
+  }
+#pragma unroll
+  for (int k = 0; k < kTsBatch; ++k) {
+    const int L = B * kTsBatch + k;
+    found |= m[k];
+    if (L & 1) p[0] |= m[k];
+    if (L & 2) p[1] |= m[k];
+    if (L & 4) p[2] |= m[k];
+    if (L & 8) p[3] |= m[k];
+  }
+}
+
+__global__ void __launch_bounds__(256) k_ms_transpose_stk(const u64 *stk, const uint32_t *stk_bm, uint32_t words,
+                                                       const uint16_t *rows, const u64 *visit, const Ctl *ctl,
+                                                       int32_t *out, int32_t V, int32_t ns) {
+  const uint32_t nst = min(ctl->level + 1, ctl->stk_levels);  // stack levels this run produced
+  const uint32_t full = ctl->stk_pull;
+  const uint32_t groups = ((uint32_t)V + 31) / 32;
+  const int lane = lane_id();
+  const uint32_t nwarps = (gridDim.x * blockDim.x) >> 5;
+  for (uint32_t grp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; grp < groups; grp += nwarps) {
+    const int64_t v = (int64_t)grp * 32 + lane;
+    const bool in = v < V;
+    const u64 vis = in ? __ldcs(&visit[v]) : 0ull;
+    u64 p[4] = {0, 0, 0, 0}, found = 0;
+    ts_fold<0>(stk, stk_bm, words, nst, full, V, grp, v, in, lane, p, found);
+    if (nst > kTsBatch) ts_fold<1>(stk, stk_bm, words, nst, full, V, grp, v, in, lane, p, found);
+    const u64 deep = vis & ~found;  // reached past the stack: depth rows
+    const bool any_deep = __any_sync(0xffffffffu, deep != 0ull);
+    int32_t *o = out + v;
+    // sources in pieces of 8 (one 16-byte piece of a depth row)
+#pragma unroll 1
+    for (int c = 0; c < 8 && 8 * c < ns; ++c) {
+      const int sh = 8 * c;
+      const uint32_t f = (uint32_t)(found >> sh), r = (uint32_t)(vis >> sh);
+      const uint32_t p0 = (uint32_t)(p[0] >> sh), p1 = (uint32_t)(p[1] >> sh);
+      const uint32_t p2 = (uint32_t)(p[2] >> sh), p3 = (uint32_t)(p[3] >> sh);
+      int4 q = make_int4(0, 0, 0, 0);
+      if (any_deep && ((deep >> sh) & 0xffull) != 0ull) q = *reinterpret_cast<const int4 *>(rows + v * 64 + sh);
+#pragma unroll
+      for (int i = 0; i < 8; ++i) {
+        if (sh + i >= ns) break;
+        int32_t d = (int32_t)(((p0 >> i) & 1u) | (((p1 >> i) & 1u) << 1) | (((p2 >> i) & 1u) << 2) |
+                              (((p3 >> i) & 1u) << 3));
+        if (!((f >> i) & 1u)) d = ((r >> i) & 1u) ? tr_entry<uint16_t>(q, i) : -1;
+        if (in) o[(int64_t)(sh + i) * V] = d;
+      }
+    }
+  }
+}
+
+// The level stack and the uint16 depth rows of a batched BFS inside multi_out.
+static u64 *stack_of(mg_graph *g) { return reinterpret_cast<u64 *>(g->multi_out); }
+static uint16_t *rows16_of(mg_graph *g) {
+  return reinterpret_cast<uint16_t *>(stack_of(g) + (size_t)kMsStackLevels * (size_t)g->csr.V);
+}
+
+// Transposes a run's results to the caller's [nsrc][V] int32 layout on stream
+// s: from the level stack and uint16 rows (stack), else from int32 rows.
+static void launch_transpose(mg_graph *g, bool stack, const u64 *visit, int32_t *out, int32_t nsrc, cudaStream_t s) {
   const int32_t V = g->csr.V;
-  const int kv = depth16 ? TrShape<uint16_t>::kV : TrShape<int32_t>::kV;
-  const unsigned nblk = (unsigned)std::min<int64_t>((int64_t)g->num_sms * 6, ((int64_t)V + kv - 1) / kv);  // 6 CTAs fit on an SM
-  if (depth16)
-    k_ms_transpose<uint16_t><<<nblk, 256, 0, s>>>(reinterpret_cast<const uint16_t *>(g->multi_out), visit, out, V, 0,
-                                                  nsrc);
+  // vertices per CTA and resident CTAs per SM (the stack variant: 8 warps of 32
+  // vertices, 48 registers; the row variant: 6 CTAs fit on an SM)
+  const int kv = stack ? 256 : TrShape<int32_t>::kV, per_sm = stack ? 5 : 6;
+  const unsigned nblk = (unsigned)std::min<int64_t>((int64_t)g->num_sms * per_sm, ((int64_t)V + kv - 1) / kv);
+  if (stack)
+    k_ms_transpose_stk<<<nblk, 256, 0, s>>>(stack_of(g), g->multi_stk_bm, (uint32_t)((V + 31) / 32), rows16_of(g),
+                                            visit, g->ws.ctl, out, V, nsrc);
   else
     k_ms_transpose<int32_t><<<nblk, 256, 0, s>>>(g->multi_out, visit, out, V, 0, nsrc);
   count_launch();
@@ -900,6 +1056,10 @@ static MultiArgs multi_args(mg_graph *g) {
   a.F0 = g->mask[1];
   a.F1 = g->mask[2];
   a.out = g->multi_out;
+  a.rows = g->multi_out;
+  a.stk = nullptr;
+  a.stk_bm = g->multi_stk_bm;
+  a.stk_words = (uint32_t)((g->csr.V + 31) / 32);
   a.q0 = g->ws.queue[0];
   a.q1 = g->ws.queue[1];
   a.bm0 = g->ws.bm[0];
@@ -911,7 +1071,7 @@ static MultiArgs multi_args(mg_graph *g) {
 }
 
 static int multi_prepare(mg_graph *g, const int32_t *srcs, int32_t nsrc, const mg_options *o, cudaStream_t s,
-                         SrcList *list, int32_t fill) {
+                         SrcList *list, int32_t fill, bool stack = false) {
   if (nsrc < 1 || nsrc > 64) return set_error(MG_ERR_ARG, "nsrc must be in [1, 64]");
   std::vector<int32_t> distinct;
   int st = check_sources(g, srcs, nsrc, &distinct);
@@ -930,6 +1090,9 @@ static int multi_prepare(mg_graph *g, const int32_t *srcs, int32_t nsrc, const m
   if (e == cudaSuccess) e = cudaMemsetAsync(g->mask[2], 0, V * 8, s);
   if (e == cudaSuccess) e = cudaMemsetAsync(g->ws.bm[0], 0, g->ws.words * 4, s);
   if (e == cudaSuccess) e = cudaMemsetAsync(g->ws.bm[1], 0, g->ws.words * 4, s);
+  // valid-entry bitmaps of the stack levels a push makes
+  if (e == cudaSuccess && stack)
+    e = cudaMemsetAsync(g->multi_stk_bm, 0, (size_t)kMsStackLevels * ((V + 31) / 32) * 4, s);
   if ((st = cuda_status(e, "batched init")) != MG_OK) return st;
   // batched BFS leaves the depth rows unset: the visit masks say which entries
   // were written; batched SSSP relaxes with atomicMin from `fill`
@@ -944,13 +1107,13 @@ static int multi_prepare(mg_graph *g, const int32_t *srcs, int32_t nsrc, const m
 // Device output: the transpose runs as the level loop's epilogue, before the
 // control block is read back.
 static std::function<void(cudaStream_t)> transpose_epilogue(mg_graph *g, int32_t nsrc, int32_t *out, bool bfs,
-                                                            bool depth16) {
+                                                            bool stack) {
   const u64 *visit = bfs ? g->mask[0] : nullptr;
-  return [=](cudaStream_t ss) { launch_transpose(g, depth16, visit, out, nsrc, ss); };
+  return [=](cudaStream_t ss) { launch_transpose(g, stack, visit, out, nsrc, ss); };
 }
 
 static int multi_finish(mg_graph *g, cudaStream_t s, int32_t nsrc, int32_t *out, int32_t unreached, mg_stats *stats,
-                        const mg_options *o, const LoopResult &res, bool depth16) {
+                        const mg_options *o, const LoopResult &res, bool stack) {
   finish_run(g, res.ctl.level);
   if (res.ctl.error) return set_error(res.ctl.error, std::string("batched traversal: device reported ") +
                                                          mg_status_string(res.ctl.error));
@@ -991,7 +1154,7 @@ static int multi_finish(mg_graph *g, cudaStream_t s, int32_t nsrc, int32_t *out,
   // Host output: transpose every source into a device staging buffer (kept for
   // later runs), then one copy to the caller.
   if (!g->multi_stage && (st = device_alloc(g, (void **)&g->multi_stage, (size_t)V * 64 * 4)) != MG_OK) return st;
-  launch_transpose(g, depth16, visit, g->multi_stage, nsrc, s);
+  launch_transpose(g, stack, visit, g->multi_stage, nsrc, s);
   cudaError_t e = cudaMemcpyAsync(out, g->multi_stage, (size_t)nsrc * V * 4, cudaMemcpyDeviceToHost, s);
   if (e == cudaSuccess) e = cudaStreamSynchronize(s);
   return cuda_status(e, "batched result copy");
@@ -1007,8 +1170,10 @@ static const mg_options *opts_or_default(const mg_options *o, mg_options *d) {
   return d;
 }
 
-// One batched BFS with DT depth rows. A uint16 run stops after level
-// kMsDepth16Levels; *depth_overflow then tells the caller to rerun with int32.
+// One batched BFS: with DT = uint16_t the level stack plus uint16 depth rows
+// past it, with DT = int32_t int32 depth rows only. A uint16 run stops after
+// level kMsDepth16Levels; *depth_overflow then tells the caller to rerun with
+// int32.
 template <typename DT>
 static int bfs_multi_run(mg_graph *g, const int32_t *srcs, int32_t nsrc, int32_t *depths, mg_stats *stats,
                          const mg_options *o, bool *depth_overflow) {
@@ -1016,15 +1181,20 @@ static int bfs_multi_run(mg_graph *g, const int32_t *srcs, int32_t nsrc, int32_t
   *depth_overflow = false;
   cudaStream_t s = run_stream(g, o);
   SrcList list;
-  int st = multi_prepare(g, srcs, nsrc, o, s, &list, -1);
+  int st = multi_prepare(g, srcs, nsrc, o, s, &list, -1, d16);
   if (st != MG_OK) return st;
   MultiArgs a = multi_args(g);
   a.all = (nsrc == 64) ? ~0ull : ((1ull << nsrc) - 1);
+  if (d16) {
+    a.stk = stack_of(g);
+    a.rows = rows16_of(g);
+  }
   GasArgs<msbfs_push> ga;
   ga.g = g->csr;
   ga.vl.visit = a.visit;
   ga.vl.F0 = a.F0;
   ga.vl.F1 = a.F1;
+  ga.vl.stk = a.stk;
   ga.el.nodes = (int)g->nodes;
   ga.queue0 = g->ws.queue[0];
   ga.queue1 = g->ws.queue[1];

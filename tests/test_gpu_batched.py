@@ -33,14 +33,23 @@ def test_bfs_multi_rmat(scale, ef, nsrc):
         assert st["edges_traversed"] == int((reached * deg[None, :]).sum())
 
 
-def test_bfs_multi_road_grid_and_duplicate_sources():
+# direction policies of a deep traversal: push and pull levels before and past
+# the 16 levels whose masks the level stack keeps; the last one flips between
+# push and pull whenever the frontier grows or shrinks
+ROAD_MODES = [dict(direction=d) for d in DIRS] + [dict(direction=_lib.MG_DIR_AUTO, alpha_multi=1e9, beta=0.5)]
+
+
+@pytest.mark.parametrize("mode", ROAD_MODES)
+def test_bfs_multi_road_grid_and_duplicate_sources(mode):
     hg = HostGraph.road_grid(150, 0.02, 0.005, seed=5)
     g = Graph(hg)
     srcs = np.array([0, 11249, 22499, 0, 500] + list(range(1000, 1059)), np.int32)  # 64, with a duplicate
-    out, st = g.bfs_multi(srcs)
+    out, st = g.bfs_multi(srcs, **mode)
     ref = np.stack([oracle.bfs(hg.row_offsets, hg.column_indices, s) for s in srcs])
     assert np.array_equal(out, ref)
     assert st["iterations"] >= int(ref.max())
+    if mode.get("beta") == 0.5:
+        assert st["push_iterations"] > 2 and st["pull_iterations"] > 2
 
 
 def test_bfs_multi_directed():
