@@ -711,13 +711,17 @@ __global__ void __launch_bounds__(256, 6) k_ms_transpose(const T *in, const u64 
 // its bitmap says so), else, for levels past the stack, the uint16 depth row;
 // -1 where the visit mask lacks bit s. The stack's extent comes from the
 // control block, so the kernel can run as the level loop's epilogue.
-// A warp takes 32 consecutive vertices, one per lane: it loads the valid-entry
-// words and then the masks of up to eight levels at once, folds them into
-// four bit planes of the depth (bit b of plane b set for source s when bit b of
-// its level is set) and the found mask, and then writes the group's entries
-// source by source as 128-byte coalesced stores, each entry taken from the
-// planes with constant shifts. The depth rows are read only by lanes whose
-// vertex has sources reached past the stack.
+//
+// A warp takes 32 consecutive vertices, one per lane. It loads the valid-entry
+// words and then the masks of up to eight levels at once and folds them into
+// four bit planes of the depth (plane b holds source s when bit b of its level
+// is set) and the found mask. Each lane then turns the planes into depth bytes,
+// four sources at a time (a 4-bit piece of a plane times 0x00204081 puts its
+// bits 8 apart, as the four partial products do not overlap; sources not found
+// get 0xff), and stores them into the warp's [64][32] byte tile in shared
+// memory; the tile leaves as 16-byte stores of four vertices of one source,
+// each byte sign-extended (0xff -> -1), a 128-byte row segment per source.
+// Sources reached past the stack are rewritten from the depth rows afterwards.
 constexpr int kTsBatch = 8;  // stack levels whose loads are in flight together
 static_assert(kMsStackLevels == 2 * kTsBatch, "two load batches cover the stack");
 
@@ -748,13 +752,21 @@ MG_DEVINL void ts_fold(const u64 *stk, const uint32_t *stk_bm, uint32_t words, u
   }
 }
 
+// bits 0..3 of x moved to bits 0, 8, 16, 24
+MG_DEVINL uint32_t spread4(uint32_t x) { return ((x & 0xfu) * 0x00204081u) & 0x01010101u; }
+// byte k of x as a signed value
+MG_DEVINL int32_t sbyte(uint32_t x, int k) { return (int32_t)(int8_t)(uint8_t)(x >> (8 * k)); }
+
 __global__ void __launch_bounds__(256) k_ms_transpose_stk(const u64 *stk, const uint32_t *stk_bm, uint32_t words,
                                                        const uint16_t *rows, const u64 *visit, const Ctl *ctl,
                                                        int32_t *out, int32_t V, int32_t ns) {
+  __shared__ uint32_t tile[kNW][64][8];  // per warp: [source][32 vertices as 8 words of 4 depth bytes]
   const uint32_t nst = min(ctl->level + 1, ctl->stk_levels);  // stack levels this run produced
   const uint32_t full = ctl->stk_pull;
   const uint32_t groups = ((uint32_t)V + 31) / 32;
-  const int lane = lane_id();
+  const int lane = lane_id(), warp = warp_id();
+  const bool vec = (V & 3) == 0;  // every source row starts 16-byte aligned
+  uint8_t *tb = reinterpret_cast<uint8_t *>(tile[warp]);
   const uint32_t nwarps = (gridDim.x * blockDim.x) >> 5;
   for (uint32_t grp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; grp < groups; grp += nwarps) {
     const int64_t v = (int64_t)grp * 32 + lane;
@@ -763,27 +775,47 @@ __global__ void __launch_bounds__(256) k_ms_transpose_stk(const u64 *stk, const 
     u64 p[4] = {0, 0, 0, 0}, found = 0;
     ts_fold<0>(stk, stk_bm, words, nst, full, V, grp, v, in, lane, p, found);
     if (nst > kTsBatch) ts_fold<1>(stk, stk_bm, words, nst, full, V, grp, v, in, lane, p, found);
-    const u64 deep = vis & ~found;  // reached past the stack: depth rows
-    const bool any_deep = __any_sync(0xffffffffu, deep != 0ull);
-    int32_t *o = out + v;
-    // sources in pieces of 8 (one 16-byte piece of a depth row)
-#pragma unroll 1
-    for (int c = 0; c < 8 && 8 * c < ns; ++c) {
-      const int sh = 8 * c;
-      const uint32_t f = (uint32_t)(found >> sh), r = (uint32_t)(vis >> sh);
-      const uint32_t p0 = (uint32_t)(p[0] >> sh), p1 = (uint32_t)(p[1] >> sh);
-      const uint32_t p2 = (uint32_t)(p[2] >> sh), p3 = (uint32_t)(p[3] >> sh);
-      int4 q = make_int4(0, 0, 0, 0);
-      if (any_deep && ((deep >> sh) & 0xffull) != 0ull) q = *reinterpret_cast<const int4 *>(rows + v * 64 + sh);
 #pragma unroll
-      for (int i = 0; i < 8; ++i) {
-        if (sh + i >= ns) break;
-        int32_t d = (int32_t)(((p0 >> i) & 1u) | (((p1 >> i) & 1u) << 1) | (((p2 >> i) & 1u) << 2) |
-                              (((p3 >> i) & 1u) << 3));
-        if (!((f >> i) & 1u)) d = ((r >> i) & 1u) ? tr_entry<uint16_t>(q, i) : -1;
-        if (in) o[(int64_t)(sh + i) * V] = d;
+    for (int hf = 0; hf < 2; ++hf) {
+      const uint32_t q0 = (uint32_t)(p[0] >> (32 * hf)), q1 = (uint32_t)(p[1] >> (32 * hf));
+      const uint32_t q2 = (uint32_t)(p[2] >> (32 * hf)), q3 = (uint32_t)(p[3] >> (32 * hf));
+      const uint32_t nf = ~(uint32_t)(found >> (32 * hf));
+#pragma unroll
+      for (int w = 0; w < 8; ++w) {
+        const int sh = 4 * w;
+        const uint32_t b = spread4(q0 >> sh) | (spread4(q1 >> sh) << 1) | (spread4(q2 >> sh) << 2) |
+                           (spread4(q3 >> sh) << 3) | (spread4(nf >> sh) * 0xffu);
+        const int s0 = 32 * hf + sh;
+#pragma unroll
+        for (int k = 0; k < 4; ++k) tb[(s0 + k) * 32 + lane] = (uint8_t)(b >> (8 * k));
       }
     }
+    __syncwarp();
+    // lane l writes vertices 4(l%8) .. 4(l%8)+3 of sources l/8, l/8+4, ...
+    const int64_t vb = (int64_t)grp * 32 + 4 * (lane & 7);
+#pragma unroll 4
+    for (int s = lane >> 3; s < ns; s += 4) {
+      const uint32_t x = tile[warp][s][lane & 7];
+      int32_t *o = out + (int64_t)s * V + vb;
+      if (vec && vb + 3 < V) {
+        *reinterpret_cast<int4 *>(o) = make_int4(sbyte(x, 0), sbyte(x, 1), sbyte(x, 2), sbyte(x, 3));
+      } else {
+#pragma unroll
+        for (int k = 0; k < 4; ++k)
+          if (vb + k < V) o[k] = sbyte(x, k);
+      }
+    }
+    // sources reached past the stack: their depths from the rows, over the -1
+    // just written (ordered after it by the warp barrier)
+    const u64 deep = vis & ~found;
+    if (__any_sync(0xffffffffu, deep != 0ull)) {
+      __syncwarp();
+      for (u64 x = deep; x; x &= x - 1) {
+        const int s = __ffsll((long long)x) - 1;
+        if (s < ns) out[(int64_t)s * V + v] = (int32_t)rows[v * 64 + s];
+      }
+    }
+    __syncwarp();  // the tile is rewritten by the next group
   }
 }
 
@@ -798,8 +830,8 @@ static uint16_t *rows16_of(mg_graph *g) {
 static void launch_transpose(mg_graph *g, bool stack, const u64 *visit, int32_t *out, int32_t nsrc, cudaStream_t s) {
   const int32_t V = g->csr.V;
   // vertices per CTA and resident CTAs per SM (the stack variant: 8 warps of 32
-  // vertices, 48 registers; the row variant: 6 CTAs fit on an SM)
-  const int kv = stack ? 256 : TrShape<int32_t>::kV, per_sm = stack ? 5 : 6;
+  // vertices, 64 registers; the row variant: 6 CTAs fit on an SM)
+  const int kv = stack ? 256 : TrShape<int32_t>::kV, per_sm = stack ? 4 : 6;
   const unsigned nblk = (unsigned)std::min<int64_t>((int64_t)g->num_sms * per_sm, ((int64_t)V + kv - 1) / kv);
   if (stack)
     k_ms_transpose_stk<<<nblk, 256, 0, s>>>(stack_of(g), g->multi_stk_bm, (uint32_t)((V + 31) / 32), rows16_of(g),
