@@ -35,6 +35,7 @@
 
 #include <algorithm>
 #include <cstring>
+#include <type_traits>
 #include <vector>
 
 #include "algo_util.cuh"
@@ -185,10 +186,43 @@ __global__ void k_ms_init(MultiArgs a, SrcList L, int bfs) {
 
 // Start of a level. After a push level (apply_pending) the queued vertices
 // keep only their new sources (depth = level), recorded in the level stack
-// (mask and valid bit) or, past it, in the depth rows. When the previous
-// level's frontier came from a push (clear_pending), its parity masks are
-// cleared at its queue entries, so the parity array is all zero again before
-// this level's push ORs into it.
+// (mask and valid bit) or, past it, in the depth rows. A large queue is walked
+// in vertex order through the level's dedup bitmap, whose bits are exactly the
+// queued vertices (a warp per 32-vertex word: coalesced mask, visit and stack
+// accesses, the word itself copied as the stack level's valid bits); a small
+// one through the queue. When the previous level's frontier came from a push
+// (clear_pending), its parity masks are cleared at its queue entries (through
+// its dedup bitmap when that level ran as a pull), so the parity array is all
+// zero again before this level's push ORs into it.
+template <typename DT>
+MG_DEVINL void ms_apply_vertex(const MultiArgs &a, int v, u64 *Fc, u64 *Sk, uint32_t L, u64 &nb, u64 &act,
+                               unsigned long long &my_bytes) {
+  const u64 vis = a.visit[v];
+  nb = Fc[v] & ~vis;
+  Fc[v] = nb;
+  act |= nb;
+  my_bytes += 24;  // visit and mask read, mask write
+  if (nb) {
+    a.visit[v] = vis | nb;
+    my_bytes += 8 + (Sk ? 8ull : sizeof(DT) * (unsigned long long)__popcll(nb));
+  }
+  if (Sk) Sk[v] = nb;
+}
+
+// the depth rows of the warp's vertices with new sources (lane l: sources l and l+32)
+template <typename DT>
+MG_DEVINL void ms_write_rows(const MultiArgs &a, int v, u64 nb, uint32_t L, int lane) {
+  uint32_t wv = __ballot_sync(0xffffffffu, nb != 0);
+  while (wv) {
+    const int j = __ffs(wv) - 1;
+    wv &= wv - 1;
+    const u64 m = __shfl_sync(0xffffffffu, nb, j);
+    DT *row = depth_rows<DT>(a) + (int64_t)__shfl_sync(0xffffffffu, v, j) * 64;
+    if ((m >> lane) & 1ull) row[lane] = (DT)L;
+    if ((m >> (lane + 32)) & 1ull) row[lane + 32] = (DT)L;
+  }
+}
+
 template <typename DT>
 __global__ void __launch_bounds__(kNT) k_ms_apply(MultiArgs a) {
   Ctl *ctl = a.ctl;
@@ -200,46 +234,67 @@ __global__ void __launch_bounds__(kNT) k_ms_apply(MultiArgs a) {
   const int32_t *Q = cur_Q(a, L), *Qp = nxt_Q(a, L);
   u64 *Sk = to_stk ? stk_level(a, L) : nullptr;
   uint32_t *Sb = to_stk ? a.stk_bm + (size_t)L * a.stk_words : nullptr;
+  const uint32_t V = (uint32_t)a.g.V, words = (V + 31) / 32;
   u64 act = 0;
   unsigned long long my_bytes = 0;
   const int lane = lane_id();
-  // whole warps walk the queue, so each new vertex's depth row can be written
-  // by the warp together (lane l: sources l and l+32)
-  const uint32_t n_pad = (n + 31) & ~31u;
-  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n_pad; i += gridDim.x * blockDim.x) {
-    int v = -1;
-    u64 nb = 0;
-    if (i < n) {
-      v = Q[i];
-      const u64 vis = a.visit[v];
-      nb = Fc[v] & ~vis;
-      Fc[v] = nb;
-      act |= nb;
-      my_bytes += 28;  // queue entry, visit and mask read, mask write
-      if (nb) {
-        a.visit[v] = vis | nb;
-        my_bytes += 8 + (to_stk ? 12ull : sizeof(DT) * (unsigned long long)__popcll(nb));
-      }
-      if (to_stk) {
-        Sk[v] = nb;
-        atomicOr(&Sb[v >> 5], 1u << (v & 31));
+  const uint32_t gwarp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, nwarps = (gridDim.x * blockDim.x) >> 5;
+  if (n >= words / 8) {
+    const uint32_t *B = (L & 1) ? a.bm1 : a.bm0;  // the dedup bitmap the previous push filled
+    for (uint32_t c = gwarp; c * 32 < words; c += nwarps) {
+      const uint32_t w = c * 32 + lane;
+      const uint32_t bits = w < words ? B[w] : 0u;
+      my_bytes += w < words ? 4 : 0;
+      if (Sb && bits) Sb[w] = bits;
+      uint32_t nz = __ballot_sync(0xffffffffu, bits != 0u);
+      while (nz) {
+        const int j = __ffs(nz) - 1;
+        nz &= nz - 1;
+        const uint32_t wb = __shfl_sync(0xffffffffu, bits, j);
+        const int v = (int)((c * 32 + j) * 32 + lane);
+        u64 nb = 0;
+        if ((wb >> lane) & 1u) ms_apply_vertex<DT>(a, v, Fc, Sk, L, nb, act, my_bytes);
+        if (!to_stk) ms_write_rows<DT>(a, v, nb, L, lane);
       }
     }
-    if (to_stk) continue;
-    uint32_t wv = __ballot_sync(0xffffffffu, nb != 0);
-    while (wv) {
-      const int j = __ffs(wv) - 1;
-      wv &= wv - 1;
-      const u64 m = __shfl_sync(0xffffffffu, nb, j);
-      DT *row = depth_rows<DT>(a) + (int64_t)__shfl_sync(0xffffffffu, v, j) * 64;
-      if ((m >> lane) & 1ull) row[lane] = (DT)L;
-      if ((m >> (lane + 32)) & 1ull) row[lane + 32] = (DT)L;
+  } else {
+    // whole warps walk the queue, so the depth rows can be written by the warp
+    const uint32_t n_pad = (n + 31) & ~31u;
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n_pad; i += gridDim.x * blockDim.x) {
+      int v = -1;
+      u64 nb = 0;
+      if (i < n) {
+        v = Q[i];
+        my_bytes += 4;
+        ms_apply_vertex<DT>(a, v, Fc, Sk, L, nb, act, my_bytes);
+        if (Sb) atomicOr(&Sb[v >> 5], 1u << (v & 31));
+      }
+      if (!to_stk) ms_write_rows<DT>(a, v, nb, L, lane);
     }
   }
   if (ctl->clear_pending) {
-    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < pn; i += gridDim.x * blockDim.x) {
-      Fp[Qp[i]] = 0;
-      my_bytes += 12;
+    if (!ctl->apply_pending && L >= 2 && pn >= words / 8) {
+      // the previous level ran as a pull, so its dedup bitmap (set by the push
+      // before it; level 0's sources have none) still holds its queue: cleared
+      // in vertex order, a warp per non-zero word writing the word's 32 entries
+      const uint32_t *B = (L & 1) ? a.bm0 : a.bm1;
+      for (uint32_t c = gwarp; c * 32 < words; c += nwarps) {
+        const uint32_t w = c * 32 + lane;
+        my_bytes += w < words ? 4 : 0;
+        uint32_t nz = __ballot_sync(0xffffffffu, w < words && B[w] != 0u);
+        while (nz) {
+          const int j = __ffs(nz) - 1;
+          nz &= nz - 1;
+          const uint32_t v = (c * 32 + j) * 32 + lane;
+          if (v < V) Fp[v] = 0;
+          my_bytes += 8;
+        }
+      }
+    } else {
+      for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < pn; i += gridDim.x * blockDim.x) {
+        Fp[Qp[i]] = 0;
+        my_bytes += 12;
+      }
     }
   }
   add_bytes(ctl, KID_MS_APPLY, my_bytes);
@@ -367,7 +422,8 @@ MG_DEVINL u64 warp_or(u64 x) {
   return x;
 }
 
-constexpr int kMsSerial = 8;  // a group whose needed lists are all this short is pulled lane by lane
+constexpr int kMsSerial = 8;  // in-edges a pulling list probes lane by lane before the group sweep
+constexpr int kMsProbeA = 2;  // of which the first probe step takes this many
 constexpr int kMsSub = 4;     // 32-edge sub-chunks whose loads are in flight together
 
 // One 32-edge sub-chunk [ck, ck+32) of a group sweep: lane i holds the
@@ -403,16 +459,21 @@ MG_DEVINL void ms_segment(u64 x, int ck, int b, int e, bool starts, bool take, u
 
 // Pull level over warp groups of 32 consecutive vertices (lane j owns vertex
 // v0+j). A vertex pulls when an active source (ctl->srcmask: a source whose
-// frontier is not empty) has not reached it yet. If every pulling list of the
-// group has at most kMsSerial in-edges, each lane loads its whole list at once.
-// Otherwise the warp sweeps the pulling lists' contiguous in-edge range in
-// rounds of kMsSub x 32 edges (coalesced row-index loads, independent mask
-// gathers, a segmented OR scan per sub-chunk); after each round it drops the
-// lists that found every missing source or ended, and resumes at the first
-// list still pulling, so the early exit of the bottom-up step is kept at round
-// granularity while the loads stay coalesced and balanced across lanes. The
-// new depths of a vertex are written by the whole warp (lane l: sources l and
-// l+32 of its 256-byte row).
+// frontier is not empty) has not reached it yet. First every pulling lane
+// probes the head of its own list, two in-edges, and a list with at most six
+// more probes those too (the lists are hub-first, so after the densest levels
+// the first in-neighbour usually carries every missing source); a list that
+// found them all or ended drops out. If lists remain, the warp sweeps their
+// contiguous in-edge range in
+// rounds of kMsSub x 32 edges from the first unprobed edge (coalesced
+// row-index loads, independent mask gathers, a segmented OR scan per
+// sub-chunk; an edge probed before may be ORed again, which changes nothing);
+// after each round it drops the lists that found every missing source or
+// ended, and resumes at the first list still pulling, so the early exit of the
+// bottom-up step is kept at round granularity while the loads stay coalesced
+// and balanced across lanes. The next masks go to the level stack; past it,
+// the new depths of a vertex are written by the whole warp (lane l: sources l
+// and l+32 of its row).
 template <typename DT>
 __global__ void __launch_bounds__(kNT, 5) k_ms_pull(MultiArgs a) {
   Ctl *ctl = a.ctl;
@@ -450,20 +511,35 @@ __global__ void __launch_bounds__(kNT, 5) k_ms_pull(MultiArgs a) {
     const bool pulls = need != 0 && e > b;
     u64 acc = 0;
     unsigned long long probes = 0;
-    if (__ballot_sync(0xffffffffu, pulls && e - b > kMsSerial) == 0u) {
-      if (pulls) {
-        int u[kMsSerial];
+    bool open = pulls;
+    int bs = b;  // first in-edge of the list not probed yet
+    // probe steps: up to N more in-edges of each list that takes part, loads in
+    // flight together
+    auto probe = [&](auto n_const, bool part) {
+      constexpr int N = decltype(n_const)::value;
+      int u[N];
 #pragma unroll
-        for (int k = 0; k < kMsSerial; ++k) u[k] = b + k < e ? __ldcs(crow + b + k) : -1;
+      for (int k = 0; k < N; ++k) u[k] = (part && bs + k < e) ? __ldcs(crow + bs + k) : -1;
 #pragma unroll
-        for (int k = 0; k < kMsSerial; ++k)
-          if (u[k] >= 0) acc |= __ldg(&Fc[u[k]]);
-        probes = (unsigned long long)(e - b);
+      for (int k = 0; k < N; ++k)
+        if (u[k] >= 0) acc |= __ldg(&Fc[u[k]]);
+      if (part) {
+        const int n = min(N, e - bs);
+        probes += (unsigned long long)n;
+        bs += n;
+        open = (acc & need) != need && bs < e;
       }
-    } else {
-      uint32_t pending = __ballot_sync(0xffffffffu, pulls);
+    };
+    constexpr int kProbeB = kMsSerial - kMsProbeA;
+    if (__any_sync(0xffffffffu, open)) probe(std::integral_constant<int, kMsProbeA>(), open);
+    // the second step finishes the short lists; the long ones go to the sweep,
+    // which would load their probed edges again
+    const bool short_rest = open && e - bs <= kProbeB;
+    if (__any_sync(0xffffffffu, short_rest)) probe(std::integral_constant<int, kProbeB>(), short_rest);
+    uint32_t pending = __ballot_sync(0xffffffffu, open);
+    if (pending) {
       const bool starts = valid && e > b;
-      int c = __shfl_sync(0xffffffffu, b, __ffs(pending) - 1);
+      int c = __shfl_sync(0xffffffffu, bs, __ffs(pending) - 1);
       for (;;) {
         // one round from c; nothing past the last pulling list is loaded
         const int lim = __shfl_sync(0xffffffffu, e, 31 - __clz(pending));
@@ -484,7 +560,7 @@ __global__ void __launch_bounds__(kNT, 5) k_ms_pull(MultiArgs a) {
         // keep the lists that still miss a source and have edges left
         pending = __ballot_sync(0xffffffffu, ((pending >> lane) & 1u) && (acc & need) != need && e > c);
         if (!pending) break;
-        c = max(c, __shfl_sync(0xffffffffu, b, __ffs(pending) - 1));
+        c = max(c, __shfl_sync(0xffffffffu, bs, __ffs(pending) - 1));
       }
     }
     my_bytes += pulls ? 8 + 12ull * probes : 0;  // offsets; row index + mask per probe
@@ -527,11 +603,15 @@ __global__ void __launch_bounds__(kNT, 5) k_ms_pull(MultiArgs a) {
 // went to the parity array for every vertex (past the level stack), that array,
 // which the push writes into next. Within the stack the parity arrays are
 // already zero: push-made entries are cleared after use (k_ms_apply).
+// A CTA takes tiles of 4096 vertices: warp w covers 512 consecutive vertices
+// with 16 coalesced mask loads in flight per lane; the queue positions follow
+// vertex order (ballots within the warp, a scan over the CTA's warps, and a
+// decoupled look-back over tiles).
+constexpr int kCvK = 16;  // vertices per lane and tile
 __global__ void __launch_bounds__(kNT) k_ms_convert(MultiArgs a) {
-  constexpr int VPT = 4;
-  constexpr uint32_t TV = kNT * VPT;
-  __shared__ uint32_t s_red[kNW + 1];
-  __shared__ uint32_t s_tile, s_prefix;
+  constexpr uint32_t TV = kNT * kCvK;
+  __shared__ uint32_t s_w[kNW];
+  __shared__ uint32_t s_tile;
   __shared__ int s_fail;
   Ctl *ctl = a.ctl;
   if (!ctl->active || !ctl->convert) return;
@@ -546,29 +626,36 @@ __global__ void __launch_bounds__(kNT) k_ms_convert(MultiArgs a) {
     a.bm1[w] = 0;
   }
   const uint32_t ntiles = (V + TV - 1) / TV;
+  const int lane = lane_id(), warp = warp_id();
   if (threadIdx.x == 0) s_fail = 0;
   for (;;) {
     const uint32_t tile = next_tile(&ctl->tile_ctr[3], &s_tile);
     if (tile >= ntiles || s_fail) break;
-    const uint32_t vb = tile * TV + threadIdx.x * VPT;
-    uint32_t flags = 0, c = 0;
+    const uint32_t wb = tile * TV + (uint32_t)warp * (32u * kCvK);  // the warp's first vertex
+    u64 f[kCvK];
 #pragma unroll
-    for (int k = 0; k < VPT; ++k) {
-      if (vb + k < V) {
-        if (Fc[vb + k]) {
-          flags |= 1u << k;
-          ++c;
-        }
-        if (Fo) Fo[vb + k] = 0;
-      }
+    for (int k = 0; k < kCvK; ++k) {
+      const uint32_t v = wb + 32u * k + lane;
+      f[k] = v < V ? Fc[v] : 0ull;
     }
-    uint32_t tot;
-    const uint32_t ex = cta_exclusive_sum(c, s_red, &tot);
-    if (warp_id() == 0) {
+    uint32_t bal[kCvK], wtot = 0;
+#pragma unroll
+    for (int k = 0; k < kCvK; ++k) {
+      bal[k] = __ballot_sync(0xffffffffu, f[k] != 0ull);
+      wtot += __popc(bal[k]);
+      const uint32_t v = wb + 32u * k + lane;
+      if (Fo && v < V) Fo[v] = 0;
+    }
+    if (lane == 0) s_w[warp] = wtot;
+    __syncthreads();
+    if (warp == 0) {
+      const uint32_t x = lane < kNW ? s_w[lane] : 0u;
+      const uint32_t inc = warp_inclusive_sum(x);
+      const uint32_t tot = __shfl_sync(0xffffffffu, inc, kNW - 1);
       bool failed = false;
       const uint32_t pre = lookback(a.status, tile, tot, epoch, ctl->spin_limit, &failed);
-      if (lane_id() == 0) {
-        s_prefix = pre;
+      if (lane < kNW) s_w[lane] = pre + inc - x;  // queue position of each warp's first vertex
+      if (lane == 0) {
         if (failed) {
           s_fail = 1;
           raise_error(ctl, MG_ERR_TIMEOUT);
@@ -579,13 +666,15 @@ __global__ void __launch_bounds__(kNT) k_ms_convert(MultiArgs a) {
     }
     __syncthreads();
     if (s_fail) break;
-    uint32_t pos = s_prefix + ex;
+    uint32_t pos = s_w[warp];
 #pragma unroll
-    for (int k = 0; k < VPT; ++k)
-      if ((flags >> k) & 1u) {
-        if (pos < V) Q[pos] = (int32_t)(vb + k);
-        ++pos;
+    for (int k = 0; k < kCvK; ++k) {
+      if ((bal[k] >> lane) & 1u) {
+        const uint32_t q = pos + __popc(bal[k] & lanemask_lt());
+        if (q < V) Q[q] = (int32_t)(wb + 32u * k + lane);
       }
+      pos += __popc(bal[k]);
+    }
   }
 }
 
