@@ -611,7 +611,8 @@ def main():
         srcs = pick_sources(ro, NSRC)
         vals, info = cpu_bfs_steps(ro, col, srcs, cpu_cores, max(1, args.steps), args.warmup)
         v = statistics.median(vals)
-        line = {"impl": "reference", "metric": metric, "value": v, "unit": "GTEPS", "n_gpus": 0,
+        # n_gpus is the launch's N (the arm runs on rank 0's host cores; cpu_baseline.cores says how many)
+        line = {"impl": "reference", "metric": metric, "value": v, "unit": "GTEPS", "n_gpus": world,
                 "steps": args.steps, "warmup": args.warmup, "higher_is_better": True, "dtype": "int32",
                 "data": "synthetic", "config": config,
                 "cpu_baseline": {"value": v, "unit": "GTEPS", "cores": cpu_cores, "kind": info["kind"],
