@@ -61,6 +61,25 @@ def test_bfs_multi_directed():
         assert np.array_equal(g.bfs_multi(srcs, direction=d)[0], ref), d
 
 
+def test_bfs_multi_runs_in_a_row():
+    # runs on one graph in a row, with a run cut short by iter_num and a batched
+    # SSSP (which shares the frontier mask arrays) in between
+    hg = HostGraph.rmat(13, 16, seed=12).with_weights(1, 20, seed=12)
+    g = Graph(hg)
+    a, b = seeded_sources(hg, 64, seed=1), seeded_sources(hg, 40, seed=2)
+    ref_a = np.stack([oracle.bfs(hg.row_offsets, hg.column_indices, s) for s in a])
+    ref_b = np.stack([oracle.bfs(hg.row_offsets, hg.column_indices, s) for s in b])
+    for _ in range(2):
+        assert np.array_equal(g.bfs_multi(a)[0], ref_a)
+        assert np.array_equal(g.bfs_multi(b)[0], ref_b)
+    cut, st = g.bfs_multi(a, iter_num=2)
+    assert st["iterations"] == 2 and not st["converged"]
+    assert np.array_equal(np.where(cut >= 0, cut, ref_a), ref_a) and (cut == -1).sum() > (ref_a == -1).sum()
+    assert np.array_equal(g.bfs_multi(b)[0], ref_b)
+    g.sssp_multi(a)
+    assert np.array_equal(g.bfs_multi(a)[0], ref_a)
+
+
 def test_bfs_multi_host_loop_equals_graph_loop():
     hg = HostGraph.rmat(13, 16, seed=2)
     g = Graph(hg)
