@@ -207,23 +207,39 @@ __global__ void __launch_bounds__(kNT, 6) k_bfs_push(GasArgs<BfsP> a) {
     uint32_t word[VT];
 #pragma unroll
     for (int r = 0; r < VT; ++r) word[r] = ((unsigned)nbr[r] < (unsigned)V) ? ld_volatile(&visited[nbr[r] >> 5]) : ~0u;
+    // the test-and-sets of all VT items in flight together, then the winners'
+    // out-degrees, then their writes and ballots (each step waits only once)
+    uint32_t surv = 0;  // bit r: item r won its test-and-set
+#pragma unroll
+    for (int r = 0; r < VT; ++r) {
+      const int u = nbr[r];
+      if ((unsigned)u < (unsigned)V) {
+        const uint32_t bit = 1u << (u & 31);
+        if (!(word[r] & bit) && !(atomicOr(&visited[u >> 5], bit) & bit)) surv |= 1u << r;
+      }
+    }
+    int d0[VT], d1[VT];
+#pragma unroll
+    for (int r = 0; r < VT; ++r) {
+      d0[r] = d1[r] = 0;
+      if ((surv >> r) & 1u) {
+        d0[r] = ro[nbr[r]];
+        d1[r] = ro[nbr[r] + 1];
+      }
+    }
     uint32_t bal[VT];
     int32_t outv[VT];
 #pragma unroll
     for (int r = 0; r < VT; ++r) {
-      bool surv = false;
       const int u = nbr[r];
-      if ((unsigned)u < (unsigned)V) {
-        const uint32_t bit = 1u << (u & 31);
-        if (!(word[r] & bit)) surv = !(atomicOr(&visited[u >> 5], bit) & bit);
-      }
-      if (surv) {
+      const bool won = (surv >> r) & 1u;
+      if (won) {
         labels[u] = (int)level + 1;
         atomicOr(&next_bm[u >> 5], 1u << (u & 31));
-        my_edges += (unsigned long long)(ro[u + 1] - ro[u]);
+        my_edges += (unsigned long long)(d1[r] - d0[r]);
         my_bytes += 8;  // queue entry + depth
       }
-      bal[r] = __ballot_sync(0xffffffffu, surv);
+      bal[r] = __ballot_sync(0xffffffffu, won);
       outv[r] = u;
     }
     if (!tile_enqueue<VT>(bal, outv, s_cnt, &s_prefix, &s_fail, ordered, a.status, tile, ntiles, epoch, spin_limit,

@@ -490,22 +490,37 @@ __global__ void __launch_bounds__(kNT) k_expand(GasArgs<P> a) {
     uint32_t probe[VT];
 #pragma unroll
     for (int r = 0; r < VT; ++r) probe[r] = fo[r] >= 0 ? ld_volatile(dedup + (fo[r] >> 5)) : ~0u;
-    uint32_t bal[VT];
-    int32_t outv[VT];
+    // the test-and-sets of all VT items in flight together, then the winners'
+    // degrees, then the ballots (each step waits only once)
+    bool surv[VT];
 #pragma unroll
     for (int r = 0; r < VT; ++r) {
-      bool surv = false;
+      surv[r] = false;
       if (fo[r] >= 0) {
         const uint32_t bit = 1u << (fo[r] & 31);
-        if (!(probe[r] & bit)) surv = !(atomicOr(dedup + (fo[r] >> 5), bit) & bit);
+        if (!(probe[r] & bit)) surv[r] = !(atomicOr(dedup + (fo[r] >> 5), bit) & bit);
       }
-      if (track_next_edges_trait<P>::value && surv) {
-        my_edges += (unsigned long long)(ro[fo[r] + 1] - ro[fo[r]]);
-        if (both) my_edges += (unsigned long long)(a.g.csc_offsets[fo[r] + 1] - a.g.csc_offsets[fo[r]]);
+    }
+    uint32_t bal[VT];
+    int32_t outv[VT];
+    if (track_next_edges_trait<P>::value) {
+      int32_t dg[VT];
+#pragma unroll
+      for (int r = 0; r < VT; ++r) {
+        dg[r] = 0;
+        if (surv[r]) {
+          dg[r] = ro[fo[r] + 1] - ro[fo[r]];
+          if (both) dg[r] += a.g.csc_offsets[fo[r] + 1] - a.g.csc_offsets[fo[r]];
+        }
       }
-      bal[r] = __ballot_sync(0xffffffffu, surv);
+#pragma unroll
+      for (int r = 0; r < VT; ++r) my_edges += (unsigned long long)dg[r];
+    }
+#pragma unroll
+    for (int r = 0; r < VT; ++r) {
+      bal[r] = __ballot_sync(0xffffffffu, surv[r]);
       outv[r] = fo[r];
-      if (surv) my_bytes += 8;  // queue entry + the Program's per-vertex write
+      if (surv[r]) my_bytes += 8;  // queue entry + the Program's per-vertex write
     }
     if (!tile_enqueue<VT>(bal, outv, s_cnt, &s_prefix, &s_fail, ordered, a.status, tile, ntiles, epoch, spin_limit,
                           Fout, (uint32_t)V, ctl))

@@ -393,13 +393,29 @@ __global__ void __launch_bounds__(kNT, 4) k_ms_push(GasArgs<msbfs_push> a) {
         my_bytes += 8;
       }
     }
-    uint32_t bal[VT];
+    // the test-and-sets of all VT items in flight together, then the winners'
+    // out-degrees, then the ballots (each step waits only once)
+    uint32_t old[VT];
 #pragma unroll
     for (int r = 0; r < VT; ++r) {
       const uint32_t bit = 1u << (head[r] & 31);
-      const bool surv = m[r] && !(probe[r] & bit) && !(atomicOr(&dedup[head[r] >> 5], bit) & bit);
+      old[r] = (m[r] && !(probe[r] & bit)) ? atomicOr(&dedup[head[r] >> 5], bit) : bit;
+    }
+    int d0[VT], d1[VT];
+#pragma unroll
+    for (int r = 0; r < VT; ++r) {
+      d0[r] = d1[r] = 0;
+      if (!(old[r] & (1u << (head[r] & 31)))) {
+        d0[r] = ro[head[r]];
+        d1[r] = ro[head[r] + 1];
+      }
+    }
+    uint32_t bal[VT];
+#pragma unroll
+    for (int r = 0; r < VT; ++r) {
+      const bool surv = !(old[r] & (1u << (head[r] & 31)));
       if (surv) {
-        my_edges += (unsigned long long)(ro[head[r] + 1] - ro[head[r]]);
+        my_edges += (unsigned long long)(d1[r] - d0[r]);
         my_bytes += 8;  // queue entry + next-mask word
       }
       bal[r] = __ballot_sync(0xffffffffu, surv);

@@ -128,17 +128,22 @@ __global__ void __launch_bounds__(kNT, 5) k_sssp_relax(GasArgs<sssp_relax> a) {
         my_bytes += 4;  // the improved distance
       }
     }
+    // the test-and-sets of all VT items in flight together, then the ballots
+    bool surv[VT];
+#pragma unroll
+    for (int r = 0; r < VT; ++r) {
+      surv[r] = false;
+      if (better[r]) {
+        const uint32_t bit = 1u << (head[r] & 31);
+        if (!(probe[r] & bit)) surv[r] = !(atomicOr(dedup + (head[r] >> 5), bit) & bit);
+      }
+    }
     uint32_t bal[VT];
     int32_t outv[VT];
 #pragma unroll
     for (int r = 0; r < VT; ++r) {
-      bool surv = false;
-      if (better[r]) {
-        const uint32_t bit = 1u << (head[r] & 31);
-        if (!(probe[r] & bit)) surv = !(atomicOr(dedup + (head[r] >> 5), bit) & bit);
-      }
-      if (surv) my_bytes += 8;  // queue entry + dedup word
-      bal[r] = __ballot_sync(0xffffffffu, surv);
+      if (surv[r]) my_bytes += 8;  // queue entry + dedup word
+      bal[r] = __ballot_sync(0xffffffffu, surv[r]);
       outv[r] = head[r];
     }
     if (!tile_enqueue<VT>(bal, outv, s_cnt, &s_prefix, &s_fail, ordered, a.status, tile, ntiles, epoch, spin_limit,
