@@ -5,6 +5,7 @@
 // distinct vertices, so V entries suffice), allocated once per graph and reused.
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <cstring>
 #include <vector>
 
@@ -90,6 +91,24 @@ int ensure_multi(mg_graph *g) {
   if (!g->multi_stk_bm &&
       (st = device_alloc(g, (void **)&g->multi_stk_bm, (size_t)kMsStackLevels * ((V + 31) / 32) * 4)) != MG_OK)
     return st;
+  if (g->ms_nheavy < 0) {
+    // the long in-lists, longest first (the pull kernel deals them to warps in
+    // this order, back and forth, so each warp gets a similar share)
+    std::vector<int32_t> off(V + 1);
+    cudaError_t e = cudaMemcpy(off.data(), g->csr.csc_offsets, (V + 1) * 4, cudaMemcpyDeviceToHost);
+    if ((st = cuda_status(e, "in-list lengths")) != MG_OK) return st;
+    std::vector<int32_t> heavy;
+    for (size_t v = 0; v < V; ++v)
+      if (off[v + 1] - off[v] > kMsHeavyList) heavy.push_back((int32_t)v);
+    std::stable_sort(heavy.begin(), heavy.end(),
+                     [&](int32_t x, int32_t y) { return off[x + 1] - off[x] > off[y + 1] - off[y]; });
+    if ((st = device_alloc(g, (void **)&g->ms_heavy, std::max<size_t>(heavy.size(), 1) * 4)) != MG_OK) return st;
+    if (!heavy.empty()) {
+      e = cudaMemcpy(g->ms_heavy, heavy.data(), heavy.size() * 4, cudaMemcpyHostToDevice);
+      if ((st = cuda_status(e, "long in-lists upload")) != MG_OK) return st;
+    }
+    g->ms_nheavy = (int32_t)heavy.size();
+  }
   return MG_OK;
 }
 

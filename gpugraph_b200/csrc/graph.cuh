@@ -30,6 +30,9 @@ namespace mg {
 // [V][64] result buffer holds them ([16][V] u64 = 128 bytes per vertex) beside
 // the uint16 depth rows (another 128 bytes per vertex).
 constexpr uint32_t kMsStackLevels = 16;
+// In-lists longer than this are pulled by a warp of their own in a batched BFS
+// pull level (a 32-vertex group holding one would carry most of a warp's work).
+constexpr int32_t kMsHeavyList = 512;
 
 struct DevCsr {
   int32_t *row_offsets = nullptr;
@@ -99,6 +102,8 @@ struct mg_graph {
   // masks), the second the [V][64] uint16 depth rows of deeper levels.
   int32_t *multi_out = nullptr;
   uint32_t *multi_stk_bm = nullptr;     // [kMsStackLevels][V/32] valid entries of push-made stack levels
+  int32_t *ms_heavy = nullptr;          // vertices with more than kMsHeavyList in-edges, longest first
+  int32_t ms_nheavy = -1;               // their number (-1: not built yet)
   int32_t *multi_stage = nullptr;       // [64][V] transposed results on their way to host memory
   size_t multi_bytes = 0;
   // PageRank plan (built on first mg_pagerank): heavy in-lists split into

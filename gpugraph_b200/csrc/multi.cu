@@ -112,6 +112,8 @@ struct MultiArgs {
   u64 *stk;           // level stack [kMsStackLevels][V], or null
   uint32_t *stk_bm;   // [kMsStackLevels][stk_words] valid entries of push-made stack levels
   uint32_t stk_words;
+  const int32_t *heavy;  // in-lists longer than kMsHeavyList, longest first
+  int32_t nheavy;
   int32_t *q0, *q1;
   uint32_t *bm0, *bm1;
   unsigned long long *status;
@@ -440,6 +442,7 @@ MG_DEVINL u64 warp_or(u64 x) {
 
 constexpr int kMsSerial = 8;  // in-edges a pulling list probes lane by lane before the group sweep
 constexpr int kMsProbeA = 2;  // of which the first probe step takes this many
+constexpr int kMsHeavyK = 4;  // loads per lane and round of a long in-list
 constexpr int kMsSub = 4;     // 32-edge sub-chunks whose loads are in flight together
 
 // One 32-edge sub-chunk [ck, ck+32) of a group sweep: lane i holds the
@@ -512,19 +515,89 @@ __global__ void __launch_bounds__(kNT, 5) k_ms_pull(MultiArgs a) {
   __shared__ unsigned long long s_tot[3];
   if (threadIdx.x < 3) s_tot[threadIdx.x] = 0;
   __syncthreads();
-  // groups are dealt round-robin over the grid's warps: an atomic ticket per
-  // group on one shared counter cost more than the imbalance it removed
+  const uint32_t nwarps = (gridDim.x * blockDim.x) >> 5, gw = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  // Long in-lists first, dealt back and forth over the warps in order of length
+  // (the groups below skip them). Lane k of a warp takes the warp's k-th list:
+  // its visit mask and, when it needs a source, its first kMsSerial in-edges
+  // (hub-first lists: usually enough once the densest level is past); the lists
+  // still open are then swept by the whole warp, one at a time, in rounds of
+  // 32 x kMsHeavyK edges (lane-local ORs, one warp OR per round for the early
+  // exit). Every long list's next mask is written here.
+  for (uint32_t k0 = 0; k0 * nwarps < (uint32_t)a.nheavy; k0 += 32) {
+    const uint32_t k = k0 + lane;
+    const uint32_t pos = k * nwarps + ((k & 1) ? nwarps - 1 - gw : gw);
+    int hv = -1, hb = 0, he = 0;
+    u64 hvis = 0, hneed = 0, hacc = 0;
+    if (k * nwarps < (uint32_t)a.nheavy && pos < (uint32_t)a.nheavy) {
+      hv = a.heavy[pos];
+      hvis = a.visit[hv];
+      hneed = active_src & ~hvis;
+      hb = coff[hv];
+      he = coff[hv + 1];
+      my_bytes += 24;  // visit, offsets, next mask
+    }
+    if (hneed) {
+      int u[kMsSerial];
+#pragma unroll
+      for (int q = 0; q < kMsSerial; ++q) u[q] = __ldcs(crow + hb + q);  // a long list has more than kMsSerial
+#pragma unroll
+      for (int q = 0; q < kMsSerial; ++q) hacc |= __ldg(&Fc[u[q]]);
+      my_bytes += 12ull * kMsSerial;
+    }
+    bool open = hneed != 0ull && (hacc & hneed) != hneed;
+    for (uint32_t todo = __ballot_sync(0xffffffffu, open); todo; todo &= todo - 1) {
+      const int j = __ffs(todo) - 1;
+      const u64 need = __shfl_sync(0xffffffffu, hneed, j);
+      const int e = __shfl_sync(0xffffffffu, he, j);
+      u64 all = __shfl_sync(0xffffffffu, hacc, j);
+      unsigned long long probes = 0;
+      for (int c = __shfl_sync(0xffffffffu, hb, j) + kMsSerial; c < e; c += 32 * kMsHeavyK) {
+        int uu[kMsHeavyK];
+#pragma unroll
+        for (int q = 0; q < kMsHeavyK; ++q) {
+          const int i = c + 32 * q + lane;
+          uu[q] = i < e ? __ldcs(crow + i) : -1;
+        }
+        u64 x = 0;
+#pragma unroll
+        for (int q = 0; q < kMsHeavyK; ++q)
+          if (uu[q] >= 0) {
+            x |= __ldg(&Fc[uu[q]]);
+            ++probes;
+          }
+        all |= ((u64)__reduce_or_sync(0xffffffffu, (uint32_t)(x >> 32)) << 32) |
+               __reduce_or_sync(0xffffffffu, (uint32_t)x);
+        if ((all & need) == need) break;
+      }
+      my_bytes += 12ull * probes;
+      if (lane == j) hacc = all;
+    }
+    const u64 hfound = hacc & hneed;
+    if (hv >= 0) {
+      Fn[hv] = hfound;
+      if (hfound) {
+        my_bytes += 8 + (to_stk ? 0ull : sizeof(DT) * (unsigned long long)__popcll(hfound));
+        a.visit[hv] = hvis | hfound;
+        my_cnt += 1;
+        my_edges += (unsigned long long)(ro[hv + 1] - ro[hv]);
+        act |= hfound;
+      }
+    }
+    if (!to_stk) ms_write_rows<DT>(a, hv, hfound, L + 1, lane);
+  }
+  // 32-vertex groups, dealt round-robin over the grid's warps: an atomic ticket
+  // per group on one shared counter cost more than the imbalance it removed
   // (batched step 2.16 vs 2.08 ms on R-MAT 22, 4.69 vs 4.42 ms on the road grid)
-  const uint32_t nwarps = (gridDim.x * blockDim.x) >> 5;
-  for (uint32_t grp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; grp < groups; grp += nwarps) {
+  for (uint32_t grp = gw; grp < groups; grp += nwarps) {
     const int v0 = (int)(grp * 32);
     const int v = v0 + lane;
     const bool valid = v < V;
     const u64 vis = valid ? a.visit[v] : ~0ull;
     const u64 need = active_src & ~vis;
     const int b = valid ? coff[v] : 0, e = valid ? coff[v + 1] : 0;
-    my_bytes += valid ? 16 : 0;  // visit read + next-mask write
-    const bool pulls = need != 0 && e > b;
+    const bool own = valid && e - b <= kMsHeavyList;  // a long list is pulled above
+    my_bytes += own ? 16 : 0;  // visit read + next-mask write
+    const bool pulls = own && need != 0 && e > b;
     u64 acc = 0;
     unsigned long long probes = 0;
     bool open = pulls;
@@ -581,7 +654,7 @@ __global__ void __launch_bounds__(kNT, 5) k_ms_pull(MultiArgs a) {
     }
     my_bytes += pulls ? 8 + 12ull * probes : 0;  // offsets; row index + mask per probe
     acc &= need;
-    if (valid) Fn[v] = acc;
+    if (own) Fn[v] = acc;
     if (acc) {
       my_bytes += 8 + (to_stk ? 0ull : sizeof(DT) * (unsigned long long)__popcll(acc));  // visit write (+ depths)
       a.visit[v] = vis | acc;
@@ -1197,6 +1270,8 @@ static MultiArgs multi_args(mg_graph *g) {
   a.stk = nullptr;
   a.stk_bm = g->multi_stk_bm;
   a.stk_words = (uint32_t)((g->csr.V + 31) / 32);
+  a.heavy = g->ms_heavy;
+  a.nheavy = std::max(g->ms_nheavy, 0);
   a.q0 = g->ws.queue[0];
   a.q1 = g->ws.queue[1];
   a.bm0 = g->ws.bm[0];
