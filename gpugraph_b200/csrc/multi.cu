@@ -687,24 +687,25 @@ __global__ void __launch_bounds__(kNT, 5) k_ms_pull(MultiArgs a) {
   if (threadIdx.x == 0 && s_tot[2]) atomicAdd(&ctl->next_edges, s_tot[2]);
 }
 
-// Pull -> push: ordered compaction of the vertices with a non-empty mask into
+// Pull -> push: compaction of the vertices with a non-empty mask into
 // the queue; clears both dedup bitmaps and, when the previous level's masks
 // went to the parity array for every vertex (past the level stack), that array,
 // which the push writes into next. Within the stack the parity arrays are
 // already zero: push-made entries are cleared after use (k_ms_apply).
 // A CTA takes tiles of 4096 vertices: warp w covers 512 consecutive vertices
-// with 16 coalesced mask loads in flight per lane; the queue positions follow
-// vertex order (ballots within the warp, a scan over the CTA's warps, and a
-// decoupled look-back over tiles).
+// with 16 coalesced mask loads in flight per lane; within a tile the queue
+// follows vertex order (ballots within the warp, a scan over the CTA's warps),
+// and each tile reserves its range with one atomic (an ordered look-back over
+// the tiles cost 12 us more per batched BFS at R-MAT 22). The last CTA to
+// finish publishes the queue length.
 constexpr int kCvK = 16;  // vertices per lane and tile
 __global__ void __launch_bounds__(kNT) k_ms_convert(MultiArgs a) {
   constexpr uint32_t TV = kNT * kCvK;
   __shared__ uint32_t s_w[kNW];
-  __shared__ uint32_t s_tile;
-  __shared__ int s_fail;
+  __shared__ uint32_t s_tile, s_last;
   Ctl *ctl = a.ctl;
   if (!ctl->active || !ctl->convert) return;
-  const uint32_t L = ctl->level, epoch = ctl->epoch + 2;
+  const uint32_t L = ctl->level;
   const uint32_t V = (uint32_t)a.g.V;
   const u64 *Fc = front_masks(a, ctl, L);
   u64 *Fo = (L - 1 >= ctl->stk_levels) ? nxt_F(a, L) : nullptr;
@@ -716,10 +717,9 @@ __global__ void __launch_bounds__(kNT) k_ms_convert(MultiArgs a) {
   }
   const uint32_t ntiles = (V + TV - 1) / TV;
   const int lane = lane_id(), warp = warp_id();
-  if (threadIdx.x == 0) s_fail = 0;
   for (;;) {
     const uint32_t tile = next_tile(&ctl->tile_ctr[3], &s_tile);
-    if (tile >= ntiles || s_fail) break;
+    if (tile >= ntiles) break;
     const uint32_t wb = tile * TV + (uint32_t)warp * (32u * kCvK);  // the warp's first vertex
     u64 f[kCvK];
 #pragma unroll
@@ -741,20 +741,12 @@ __global__ void __launch_bounds__(kNT) k_ms_convert(MultiArgs a) {
       const uint32_t x = lane < kNW ? s_w[lane] : 0u;
       const uint32_t inc = warp_inclusive_sum(x);
       const uint32_t tot = __shfl_sync(0xffffffffu, inc, kNW - 1);
-      bool failed = false;
-      const uint32_t pre = lookback(a.status, tile, tot, epoch, ctl->spin_limit, &failed);
+      uint32_t pre = 0;
+      if (lane == 0 && tot) pre = atomicAdd(&ctl->next_size, tot);
+      pre = __shfl_sync(0xffffffffu, pre, 0);
       if (lane < kNW) s_w[lane] = pre + inc - x;  // queue position of each warp's first vertex
-      if (lane == 0) {
-        if (failed) {
-          s_fail = 1;
-          raise_error(ctl, MG_ERR_TIMEOUT);
-        } else if (tile == ntiles - 1) {
-          ctl->frontier_size = pre + tot;
-        }
-      }
     }
     __syncthreads();
-    if (s_fail) break;
     uint32_t pos = s_w[warp];
 #pragma unroll
     for (int k = 0; k < kCvK; ++k) {
@@ -764,6 +756,18 @@ __global__ void __launch_bounds__(kNT) k_ms_convert(MultiArgs a) {
       }
       pos += __popc(bal[k]);
     }
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    __threadfence();
+    s_last = atomicAdd(&ctl->done_ctas[3], 1u) == gridDim.x - 1;
+  }
+  __syncthreads();
+  if (s_last && threadIdx.x == 0) {
+    __threadfence();
+    ctl->frontier_size = *(volatile uint32_t *)&ctl->next_size;
+    ctl->next_size = 0;
+    ctl->done_ctas[3] = 0;
   }
 }
 
