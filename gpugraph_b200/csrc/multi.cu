@@ -249,14 +249,40 @@ __global__ void __launch_bounds__(kNT) k_ms_apply(MultiArgs a) {
       my_bytes += w < words ? 4 : 0;
       if (Sb && bits) Sb[w] = bits;
       uint32_t nz = __ballot_sync(0xffffffffu, bits != 0u);
+      // four non-zero words per step: their visit and mask loads in flight together
       while (nz) {
-        const int j = __ffs(nz) - 1;
-        nz &= nz - 1;
-        const uint32_t wb = __shfl_sync(0xffffffffu, bits, j);
-        const int v = (int)((c * 32 + j) * 32 + lane);
-        u64 nb = 0;
-        if ((wb >> lane) & 1u) ms_apply_vertex<DT>(a, v, Fc, Sk, L, nb, act, my_bytes);
-        if (!to_stk) ms_write_rows<DT>(a, v, nb, L, lane);
+        constexpr int W = 4;
+        int v[W];
+        bool has[W];
+        u64 vis[W], fc[W];
+#pragma unroll
+        for (int q = 0; q < W; ++q) {
+          const int j = nz ? __ffs(nz) - 1 : 0;
+          const uint32_t wb = __shfl_sync(0xffffffffu, bits, j);
+          has[q] = nz != 0u && ((wb >> lane) & 1u);
+          nz &= nz - 1;
+          v[q] = (int)((c * 32 + j) * 32 + lane);
+          if (has[q]) {
+            vis[q] = a.visit[v[q]];
+            fc[q] = Fc[v[q]];
+          }
+        }
+#pragma unroll
+        for (int q = 0; q < W; ++q) {
+          u64 nb = 0;
+          if (has[q]) {
+            nb = fc[q] & ~vis[q];
+            Fc[v[q]] = nb;
+            act |= nb;
+            my_bytes += 24;  // visit and mask read, mask write
+            if (nb) {
+              a.visit[v[q]] = vis[q] | nb;
+              my_bytes += 8 + (Sk ? 8ull : sizeof(DT) * (unsigned long long)__popcll(nb));
+            }
+            if (Sk) Sk[v[q]] = nb;
+          }
+          if (!to_stk) ms_write_rows<DT>(a, v[q], nb, L, lane);
+        }
       }
     }
   } else {
@@ -348,8 +374,17 @@ __global__ void __launch_bounds__(kNT, 4) k_ms_push(GasArgs<msbfs_push> a) {
     s_fail = 0;
     s_edges = 0;
   }
-  for (;;) {
-    const uint32_t tile = next_tile(&ctl->tile_ctr[1], &s_tile);
+  // tiles: dealt statically when the next queue is unordered (tiles all cost
+  // about the same), through the atomic counter when ordered (the look-back
+  // needs every earlier tile running or done)
+  for (uint32_t st = blockIdx.x;; st += gridDim.x) {
+    uint32_t tile;
+    if (ordered) {
+      tile = next_tile(&ctl->tile_ctr[1], &s_tile);
+    } else {
+      __syncthreads();  // the previous tile's shared state has been read
+      tile = st;
+    }
     if (tile >= ntiles || s_fail) break;
     int cnt;
     if (!decode_tile<VT>(tile, ntiles, n, items, a.part, a.scan, F, ro, s_v, s_base, s_rs, s_own, &cnt,
