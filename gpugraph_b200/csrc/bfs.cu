@@ -175,8 +175,8 @@ __global__ void __launch_bounds__(kNT, 6) k_bfs_push(GasArgs<BfsP> a) {
     s_fail = 0;
     s_edges = 0;
   }
-  for (;;) {
-    const uint32_t tile = next_tile(&ctl->tile_ctr[1], &s_tile);
+  for (uint32_t k = 0;; ++k) {
+    const uint32_t tile = take_tile(&ctl->tile_ctr[1], &s_tile, ordered, k);
     if (tile >= ntiles || s_fail) break;
     int cnt;
     if (!decode_tile<VT>(tile, ntiles, n, items, a.part, a.scan, F, ro, s_v, s_base, s_rs, s_own, &cnt,

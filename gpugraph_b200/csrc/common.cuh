@@ -248,4 +248,15 @@ MG_DEVINL uint32_t next_tile(uint32_t *ctr, uint32_t *smem_slot) {
   return *smem_slot;
 }
 
+// The CTA's k-th tile of an expand level: through the atomic counter when the
+// next queue is ordered (the look-back needs every earlier tile running or
+// done), otherwise dealt statically (merge-path tiles all hold the same number
+// of items). Call from all threads with k = 0, 1, ...; begins with a barrier,
+// so the previous tile's shared state has been read.
+MG_DEVINL uint32_t take_tile(uint32_t *ctr, uint32_t *smem_slot, bool ordered, uint32_t k) {
+  if (ordered) return next_tile(ctr, smem_slot);
+  __syncthreads();
+  return blockIdx.x + k * gridDim.x;
+}
+
 }  // namespace mg

@@ -374,17 +374,8 @@ __global__ void __launch_bounds__(kNT, 4) k_ms_push(GasArgs<msbfs_push> a) {
     s_fail = 0;
     s_edges = 0;
   }
-  // tiles: dealt statically when the next queue is unordered (tiles all cost
-  // about the same), through the atomic counter when ordered (the look-back
-  // needs every earlier tile running or done)
-  for (uint32_t st = blockIdx.x;; st += gridDim.x) {
-    uint32_t tile;
-    if (ordered) {
-      tile = next_tile(&ctl->tile_ctr[1], &s_tile);
-    } else {
-      __syncthreads();  // the previous tile's shared state has been read
-      tile = st;
-    }
+  for (uint32_t k = 0;; ++k) {
+    const uint32_t tile = take_tile(&ctl->tile_ctr[1], &s_tile, ordered, k);
     if (tile >= ntiles || s_fail) break;
     int cnt;
     if (!decode_tile<VT>(tile, ntiles, n, items, a.part, a.scan, F, ro, s_v, s_base, s_rs, s_own, &cnt,
