@@ -466,8 +466,8 @@ MG_DEVINL u64 warp_or(u64 x) {
   return x;
 }
 
-constexpr int kMsSerial = 8;  // in-edges a pulling list probes lane by lane before the group sweep
-constexpr int kMsProbeA = 2;  // of which the first probe step takes this many
+constexpr int kMsSerial = 8;  // a list this short is probed whole, lane by lane, before the group sweep
+constexpr int kMsProbeA = 2;  // in-edges a longer list probes before the sweep
 constexpr int kMsHeavyK = 4;  // loads per lane and round of a long in-list
 constexpr int kMsSub = 4;     // 32-edge sub-chunks whose loads are in flight together
 
@@ -505,10 +505,10 @@ MG_DEVINL void ms_segment(u64 x, int ck, int b, int e, bool starts, bool take, u
 // Pull level over warp groups of 32 consecutive vertices (lane j owns vertex
 // v0+j). A vertex pulls when an active source (ctl->srcmask: a source whose
 // frontier is not empty) has not reached it yet. First every pulling lane
-// probes the head of its own list, two in-edges, and a list with at most six
-// more probes those too (the lists are hub-first, so after the densest levels
-// the first in-neighbour usually carries every missing source); a list that
-// found them all or ended drops out. If lists remain, the warp sweeps their
+// probes its own list in one step: a list of at most eight in-edges all of
+// them, a longer one its first two (the lists are hub-first, so after the
+// densest levels the first in-neighbour usually carries every missing source);
+// a list that found them all or ended drops out. If lists remain, the warp sweeps their
 // contiguous in-edge range in
 // rounds of kMsSub x 32 edges from the first unprobed edge (coalesced
 // row-index loads, independent mask gathers, a segmented OR scan per
@@ -630,27 +630,23 @@ __global__ void __launch_bounds__(kNT, 5) k_ms_pull(MultiArgs a) {
     int bs = b;  // first in-edge of the list not probed yet
     // probe steps: up to N more in-edges of each list that takes part, loads in
     // flight together
-    auto probe = [&](auto n_const, bool part) {
-      constexpr int N = decltype(n_const)::value;
-      int u[N];
+    // one probe step: a list of at most kMsSerial in-edges loads all of them, a
+    // longer one its first kMsProbeA (the sweep would load more probed edges
+    // again); the loads are in flight together
+    if (__any_sync(0xffffffffu, open)) {
+      const int lim = e - b <= kMsSerial ? e : b + kMsProbeA;
+      int u[kMsSerial];
 #pragma unroll
-      for (int k = 0; k < N; ++k) u[k] = (part && bs + k < e) ? __ldcs(crow + bs + k) : -1;
+      for (int k = 0; k < kMsSerial; ++k) u[k] = (open && bs + k < lim) ? __ldcs(crow + bs + k) : -1;
 #pragma unroll
-      for (int k = 0; k < N; ++k)
+      for (int k = 0; k < kMsSerial; ++k)
         if (u[k] >= 0) acc |= __ldg(&Fc[u[k]]);
-      if (part) {
-        const int n = min(N, e - bs);
-        probes += (unsigned long long)n;
-        bs += n;
+      if (open) {
+        probes += (unsigned long long)(lim - bs);
+        bs = lim;
         open = (acc & need) != need && bs < e;
       }
-    };
-    constexpr int kProbeB = kMsSerial - kMsProbeA;
-    if (__any_sync(0xffffffffu, open)) probe(std::integral_constant<int, kMsProbeA>(), open);
-    // the second step finishes the short lists; the long ones go to the sweep,
-    // which would load their probed edges again
-    const bool short_rest = open && e - bs <= kProbeB;
-    if (__any_sync(0xffffffffu, short_rest)) probe(std::integral_constant<int, kProbeB>(), short_rest);
+    }
     uint32_t pending = __ballot_sync(0xffffffffu, open);
     if (pending) {
       const bool starts = valid && e > b;
