@@ -466,7 +466,7 @@ MG_DEVINL u64 warp_or(u64 x) {
   return x;
 }
 
-constexpr int kMsSerial = 8;  // a list this short is probed whole, lane by lane, before the group sweep
+constexpr int kMsSerial = 6;  // a list this short is probed whole, lane by lane, before the group sweep
 constexpr int kMsProbeA = 2;  // in-edges a longer list probes before the sweep
 constexpr int kMsHeavyK = 4;  // loads per lane and round of a long in-list
 constexpr int kMsSub = 4;     // 32-edge sub-chunks whose loads are in flight together
@@ -505,7 +505,7 @@ MG_DEVINL void ms_segment(u64 x, int ck, int b, int e, bool starts, bool take, u
 // Pull level over warp groups of 32 consecutive vertices (lane j owns vertex
 // v0+j). A vertex pulls when an active source (ctl->srcmask: a source whose
 // frontier is not empty) has not reached it yet. First every pulling lane
-// probes its own list in one step: a list of at most eight in-edges all of
+// probes its own list in one step: a list of at most six in-edges all of
 // them, a longer one its first two (the lists are hub-first, so after the
 // densest levels the first in-neighbour usually carries every missing source);
 // a list that found them all or ended drops out. If lists remain, the warp sweeps their
@@ -520,7 +520,7 @@ MG_DEVINL void ms_segment(u64 x, int ck, int b, int e, bool starts, bool take, u
 // the new depths of a vertex are written by the whole warp (lane l: sources l
 // and l+32 of its row).
 template <typename DT>
-__global__ void __launch_bounds__(kNT, 5) k_ms_pull(MultiArgs a) {
+__global__ void __launch_bounds__(kNT, 6) k_ms_pull(MultiArgs a) {
   Ctl *ctl = a.ctl;
   if (!ctl->active || ctl->mode != MODE_BITMAP) return;
   const uint32_t L = ctl->level;
@@ -1462,8 +1462,9 @@ static int bfs_multi_run(mg_graph *g, const int32_t *srcs, int32_t nsrc, int32_t
   count_launch(2);
   if ((st = launch_check("batched bfs init")) != MG_OK) return st;
   const int grid = persistent_grid(g, o, 4);
-  // the pull kernel holds no shared memory and at most 48 registers: 40 warps per SM
-  const int pull_grid = g->num_sms * 5;
+  // the pull kernel holds no shared memory and at most 40 registers: 48 warps per
+  // SM (a few bytes spill; 10 us faster per run at R-MAT 22 than 40 warps at 48)
+  const int pull_grid = g->num_sms * 6;
   const int32_t V = g->csr.V;
   const int64_t E = g->edges;
   LevelBody body = [=](cudaStream_t ss, cudaGraphConditionalHandle h, int use_h) {
