@@ -466,8 +466,10 @@ MG_DEVINL u64 warp_or(u64 x) {
   return x;
 }
 
-constexpr int kMsSerial = 6;  // a list this short is probed whole, lane by lane, before the group sweep
-constexpr int kMsProbeA = 2;  // in-edges a longer list probes before the sweep
+// in-edges each pulling list probes lane by lane before the warp sweeps it
+// (probing lists of up to 4, 6 or 8 in-edges whole instead was 0-10 us slower
+// per run at R-MAT 22)
+constexpr int kMsProbe = 2;
 constexpr int kMsHeavyK = 4;  // loads per lane and round of a long in-list
 constexpr int kMsSub = 4;     // 32-edge sub-chunks whose loads are in flight together
 
@@ -505,11 +507,10 @@ MG_DEVINL void ms_segment(u64 x, int ck, int b, int e, bool starts, bool take, u
 // Pull level over warp groups of 32 consecutive vertices (lane j owns vertex
 // v0+j). A vertex pulls when an active source (ctl->srcmask: a source whose
 // frontier is not empty) has not reached it yet. First every pulling lane
-// probes its own list in one step: a list of at most six in-edges all of
-// them, a longer one its first two (the lists are hub-first, so after the
-// densest levels the first in-neighbour usually carries every missing source);
-// a list that found them all or ended drops out. If lists remain, the warp sweeps their
-// contiguous in-edge range in
+// probes the first two in-edges of its own list in one step (the lists are
+// hub-first, so after the densest levels the first in-neighbour usually
+// carries every missing source); a list that found them all or ended drops
+// out. If lists remain, the warp sweeps their contiguous in-edge range in
 // rounds of kMsSub x 32 edges from the first unprobed edge (coalesced
 // row-index loads, independent mask gathers, a segmented OR scan per
 // sub-chunk; an edge probed before may be ORed again, which changes nothing);
@@ -544,7 +545,7 @@ __global__ void __launch_bounds__(kNT, 6) k_ms_pull(MultiArgs a) {
   const uint32_t nwarps = (gridDim.x * blockDim.x) >> 5, gw = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   // Long in-lists first, dealt back and forth over the warps in order of length
   // (the groups below skip them). Lane k of a warp takes the warp's k-th list:
-  // its visit mask and, when it needs a source, its first kMsSerial in-edges
+  // its visit mask and, when it needs a source, its first kMsProbe in-edges
   // (hub-first lists: usually enough once the densest level is past); the lists
   // still open are then swept by the whole warp, one at a time, in rounds of
   // 32 x kMsHeavyK edges (lane-local ORs, one warp OR per round for the early
@@ -563,12 +564,12 @@ __global__ void __launch_bounds__(kNT, 6) k_ms_pull(MultiArgs a) {
       my_bytes += 24;  // visit, offsets, next mask
     }
     if (hneed) {
-      int u[kMsSerial];
+      int u[kMsProbe];
 #pragma unroll
-      for (int q = 0; q < kMsSerial; ++q) u[q] = __ldcs(crow + hb + q);  // a long list has more than kMsSerial
+      for (int q = 0; q < kMsProbe; ++q) u[q] = __ldcs(crow + hb + q);  // a long list has more than kMsProbe
 #pragma unroll
-      for (int q = 0; q < kMsSerial; ++q) hacc |= __ldg(&Fc[u[q]]);
-      my_bytes += 12ull * kMsSerial;
+      for (int q = 0; q < kMsProbe; ++q) hacc |= __ldg(&Fc[u[q]]);
+      my_bytes += 12ull * kMsProbe;
     }
     bool open = hneed != 0ull && (hacc & hneed) != hneed;
     for (uint32_t todo = __ballot_sync(0xffffffffu, open); todo; todo &= todo - 1) {
@@ -577,7 +578,7 @@ __global__ void __launch_bounds__(kNT, 6) k_ms_pull(MultiArgs a) {
       const int e = __shfl_sync(0xffffffffu, he, j);
       u64 all = __shfl_sync(0xffffffffu, hacc, j);
       unsigned long long probes = 0;
-      for (int c = __shfl_sync(0xffffffffu, hb, j) + kMsSerial; c < e; c += 32 * kMsHeavyK) {
+      for (int c = __shfl_sync(0xffffffffu, hb, j) + kMsProbe; c < e; c += 32 * kMsHeavyK) {
         int uu[kMsHeavyK];
 #pragma unroll
         for (int q = 0; q < kMsHeavyK; ++q) {
@@ -628,18 +629,15 @@ __global__ void __launch_bounds__(kNT, 6) k_ms_pull(MultiArgs a) {
     unsigned long long probes = 0;
     bool open = pulls;
     int bs = b;  // first in-edge of the list not probed yet
-    // probe steps: up to N more in-edges of each list that takes part, loads in
-    // flight together
-    // one probe step: a list of at most kMsSerial in-edges loads all of them, a
-    // longer one its first kMsProbeA (the sweep would load more probed edges
-    // again); the loads are in flight together
+    // one probe step: the first kMsProbe in-edges of every list that takes
+    // part, the loads in flight together
     if (__any_sync(0xffffffffu, open)) {
-      const int lim = e - b <= kMsSerial ? e : b + kMsProbeA;
-      int u[kMsSerial];
+      const int lim = min(e, b + kMsProbe);
+      int u[kMsProbe];
 #pragma unroll
-      for (int k = 0; k < kMsSerial; ++k) u[k] = (open && bs + k < lim) ? __ldcs(crow + bs + k) : -1;
+      for (int k = 0; k < kMsProbe; ++k) u[k] = (open && bs + k < lim) ? __ldcs(crow + bs + k) : -1;
 #pragma unroll
-      for (int k = 0; k < kMsSerial; ++k)
+      for (int k = 0; k < kMsProbe; ++k)
         if (u[k] >= 0) acc |= __ldg(&Fc[u[k]]);
       if (open) {
         probes += (unsigned long long)(lim - bs);
@@ -973,8 +971,14 @@ __global__ void __launch_bounds__(256) k_ms_transpose_stk(const u64 *stk, const 
   const int lane = lane_id(), warp = warp_id();
   const bool vec = (V & 3) == 0;  // every source row starts 16-byte aligned
   uint8_t *tb = reinterpret_cast<uint8_t *>(tile[warp]);
-  const uint32_t nwarps = (gridDim.x * blockDim.x) >> 5;
-  for (uint32_t grp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; grp < groups; grp += nwarps) {
+  // The CTA takes 8 consecutive groups at a time and its warps start each step
+  // together, so the grid's stores move through every source row as one narrow
+  // front (with the warps on their own, about 6 us slower per run at R-MAT 22;
+  // four consecutive groups per warp, a wider front, 35 us slower).
+  for (uint32_t base = blockIdx.x * kNW; base < groups; base += gridDim.x * kNW) {
+    __syncthreads();  // every warp of the CTA runs the same steps
+    const uint32_t grp = base + warp;
+    if (grp >= groups) continue;
     const int64_t v = (int64_t)grp * 32 + lane;
     const bool in = v < V;
     const u64 vis = in ? __ldcs(&visit[v]) : 0ull;
@@ -1036,7 +1040,8 @@ static uint16_t *rows16_of(mg_graph *g) {
 static void launch_transpose(mg_graph *g, bool stack, const u64 *visit, int32_t *out, int32_t nsrc, cudaStream_t s) {
   const int32_t V = g->csr.V;
   // vertices per CTA and resident CTAs per SM (the stack variant: 8 warps of 32
-  // vertices, 64 registers; the row variant: 6 CTAs fit on an SM)
+  // vertices, 64 registers, 4 CTAs per SM: 2 leave too few loads in flight, 60 us
+  // more per run at R-MAT 22, and 3 were no faster; the row variant: 6 CTAs fit)
   const int kv = stack ? 256 : TrShape<int32_t>::kV, per_sm = stack ? 4 : 6;
   const unsigned nblk = (unsigned)std::min<int64_t>((int64_t)g->num_sms * per_sm, ((int64_t)V + kv - 1) / kv);
   if (stack)
