@@ -1,5 +1,5 @@
-// Autotuner for the level-loop launch parameters (north_star: "the expand
-// thresholds and tile shapes chosen by an autotuner the project writes").
+// Autotuner for the level-loop launch parameters: the expand thresholds, tile
+// shapes and direction-switch factors, chosen on the caller's graph.
 // The reference fixes them at compile time (KernelPolicy<..., 200>, CTA/warp
 // gather thresholds 512/32: GASengine/enactor_vertex_centric.cuh:3934-3970).
 //

@@ -1,4 +1,4 @@
-// Direction-optimising BFS (north_star (c)): push levels run the bfs Program's
+// Direction-optimising BFS (push/pull switching): push levels run the bfs Program's
 // expand + contract (Algorithms/BFS/bfs.h:28-298) fused into k_bfs_push over a
 // vertex queue; pull levels run a bottom-up sweep in which every unvisited
 // vertex scans its in-edges (hubs first) for a parent in the frontier bitmap

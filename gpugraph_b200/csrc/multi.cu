@@ -1,5 +1,5 @@
 // Batched traversal: up to 64 BFS or SSSP sources in one pass, carried as a
-// 64-bit mask per vertex (north_star "batching"). The reference runs sources
+// 64-bit mask per vertex. The reference runs sources
 // one after the other (Algorithms/BFS/bfs.cu:865-881, Algorithms/SSSP/sssp.cu:389-404);
 // here one sweep over an edge serves every source whose frontier contains its
 // tail, so the column indices are read once per level instead of once per

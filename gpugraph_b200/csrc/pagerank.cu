@@ -1,4 +1,4 @@
-// Normalised PageRank as a pull SpMV over the transposed graph (north_star (e)),
+// Normalised PageRank as a pull SpMV over the transposed graph,
 // replacing the reference's gather_mgpu + ReduceByKey pipeline
 // (GASengine/enactor_vertex_centric.cuh:2104-2725, mgpukernel/kernel.cuh:300-404),
 // which writes and re-reads (dst, value) pairs for every edge.
@@ -432,7 +432,7 @@ extern "C" int mg_pagerank(mg_graph *g, float *ranks, mg_stats *stats, const mg_
   if ((st = pr_plan(g, s)) != MG_OK) return st;
   const int32_t V = g->csr.V;
   const double d = o->damping, inv_n = 1.0 / (double)V;
-  // the reference's iteration cap knob; the BASELINE specification stops at 100
+  // the reference's iteration cap knob (iter_num), clamped to 2^20
   const uint32_t max_iter = (uint32_t)std::max<int32_t>(0, std::min<int32_t>(o->iter_num, 1 << 20));
   PrArgs a;
   a.coff = g->pr_coff;

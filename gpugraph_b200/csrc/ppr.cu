@@ -1,5 +1,6 @@
-// Personalised PageRank with its adjoint (no reference counterpart; north_star
-// "differentiation").
+// Personalised PageRank with its adjoint (no reference counterpart): the
+// forward solve and the gradients of a loss with respect to the teleport
+// vectors and the edge weights.
 //
 // Forward:  R = (1-d) T + d P^T R,  R, T in [V][nvec] (row-major), P[u,v] = w(e(u,v))
 //           solved by power iteration pulled over the in-edges (CSC):

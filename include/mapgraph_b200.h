@@ -42,7 +42,7 @@ enum {
 /* Edge value types for mg_graph_create (reference: CsrGraph::edge_values, Value). */
 enum { MG_VAL_NONE = 0, MG_VAL_I32 = 1, MG_VAL_F32 = 2 };
 
-/* Traversal direction policy for BFS (north_star (c): push/pull switching). */
+/* Traversal direction policy for BFS (push/pull switching). */
 enum { MG_DIR_AUTO = 0, MG_DIR_PUSH = 1, MG_DIR_PULL = 2 };
 
 typedef struct mg_graph mg_graph; /* device-resident CsrProblem (opaque) */

@@ -4,8 +4,8 @@ ctypes access to (1) the plain-C restatement of the reference's CPU algorithms
 (oracle/libmg_oracle.so, from mg_oracle.c) and (2) the reference's own CPU
 functions compiled from its sources (oracle/_ref/libref_cpu.so, from
 build_ref.sh), when present. Only tests/, __graft_entry__.smoke() and
-bench.py's CPU-baseline leg use this package, and only as the checker or the
-timed CPU baseline; the product path never imports it.
+bench.py's CPU-baseline leg use this package, and only to check results or as
+the timed CPU baseline; the product path never imports it.
 """
 from __future__ import annotations
 

@@ -7,8 +7,7 @@ from it by oracle/build_ref.sh; both read its location from $MG_REFERENCE):
 
 Each fixture stores a small graph (derived CSR arrays, not the reference's
 files) together with the outputs of CPUBFS / CPUSSSP / CPUCC / CPUPR on it, so
-the GPU box (where the reference tree does not exist) can check parity
-against them. R-MAT fixtures store only a SHA-256 of the CSR the seeded builder
+a machine without the reference tree can check parity against them. R-MAT fixtures store only a SHA-256 of the CSR the seeded builder
 must reproduce, plus the expected outputs.
 """
 from __future__ import annotations

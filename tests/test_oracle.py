@@ -25,7 +25,7 @@ def test_oracle_matches_golden(name):
 
 
 def test_known_answers_small_mtx():
-    # SURVEY-recorded outputs of the reference CPU code on smallRegressionGraphs/small.mtx from vertex 0.
+    # Known answers: the reference CPU code's outputs on smallRegressionGraphs/small.mtx from vertex 0.
     fx = load_fixture("mtx_small.json")
     assert fx["expected"]["bfs"]["0"] == [0, 1, 1, 1, 2, 2, 2]
     assert fx["expected"]["sssp"]["0"] == [0, 1, 4, 1, 2, 2, 2]
