@@ -80,6 +80,25 @@ def test_bfs_multi_runs_in_a_row():
     assert np.array_equal(g.bfs_multi(a)[0], ref_a)
 
 
+@pytest.mark.parametrize("extra", [1, 2, 3])
+def test_multi_vertex_count_not_a_multiple_of_four(extra):
+    # an R-MAT graph with 1-3 isolated vertices appended: the results leave in
+    # [nsrc][V] rows that do not start 16-byte aligned, and the last 32-vertex
+    # group and the last step of the transpose's CTAs are partial
+    base = HostGraph.rmat(11, 8, seed=17).with_weights(1, 30, seed=17)
+    ro = np.concatenate([base.row_offsets, np.full(extra, base.row_offsets[-1], np.int32)])
+    hg = HostGraph(ro, base.column_indices, base.edge_values)
+    assert hg.nodes % 4 == extra
+    g = Graph(hg)
+    srcs = np.concatenate([seeded_sources(hg, 20, seed=extra), [hg.nodes - 1]]).astype(np.int32)
+    ref = np.stack([oracle.bfs(hg.row_offsets, hg.column_indices, s) for s in srcs])
+    for d in DIRS:
+        assert np.array_equal(g.bfs_multi(srcs, direction=d)[0], ref), d
+    out, _ = g.sssp_multi(srcs)
+    for k in (0, 7, len(srcs) - 1):
+        assert np.array_equal(out[k], oracle.sssp(hg.row_offsets, hg.column_indices, hg.edge_values, srcs[k])), k
+
+
 def test_bfs_multi_host_loop_equals_graph_loop():
     hg = HostGraph.rmat(13, 16, seed=2)
     g = Graph(hg)
