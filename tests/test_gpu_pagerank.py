@@ -39,6 +39,17 @@ def test_pagerank_directed_rmat(scale, ef, seed):
     _check(hg, True)
 
 
+@pytest.mark.parametrize("extra", [1, 2, 3])
+def test_pagerank_vertex_count_not_a_multiple_of_four(extra):
+    # isolated vertices appended (dangling, no in-edges): the last 32-vertex
+    # group of the pull is partial and the vertex count is not a multiple of 4
+    base = HostGraph.rmat(12, 8, seed=21, symmetrize=False)
+    ro = np.concatenate([base.row_offsets, np.full(extra, base.row_offsets[-1], np.int32)])
+    hg = HostGraph(ro, base.column_indices)
+    assert hg.nodes % 4 == extra
+    _check(hg, True)
+
+
 def test_pagerank_road_grid_symmetric():
     hg = HostGraph.road_grid(300, 0.02, 0.005, seed=3)
     _check(hg, False)

@@ -120,6 +120,26 @@ def test_sssp_road_grid():
     assert np.array_equal(dist, oracle.sssp(hg.row_offsets, hg.column_indices, hg.edge_values, 20100))
 
 
+@pytest.mark.parametrize("extra", [1, 3])
+def test_vertex_count_not_a_multiple_of_four(extra):
+    # isolated vertices appended to an R-MAT graph: bitmaps, 32-vertex groups
+    # and 16-byte offset loads end part-way; BFS from the hub and from an
+    # appended vertex, SSSP and union-find CC against the oracle
+    base = HostGraph.rmat(12, 8, seed=23).with_weights(1, 50, seed=23)
+    ro = np.concatenate([base.row_offsets, np.full(extra, base.row_offsets[-1], np.int32)])
+    hg = HostGraph(ro, base.column_indices, base.edge_values)
+    assert hg.nodes % 4 == extra
+    g = Graph(hg)
+    hub = int(hg.max_degree_vertex())
+    for s in (hub, hg.nodes - 1):
+        for d in DIRS:
+            assert np.array_equal(g.bfs(s, direction=d)[0], oracle.bfs(hg.row_offsets, hg.column_indices, s)), (s, d)
+    dist, _ = g.sssp(hub)
+    assert np.array_equal(dist, oracle.sssp(hg.row_offsets, hg.column_indices, hg.edge_values, hub))
+    labels, _ = g.cc()
+    assert np.array_equal(labels, oracle.cc(hg.row_offsets, hg.column_indices))
+
+
 @pytest.mark.parametrize("scale,ef", [(16, 16), (14, 2)])
 def test_cc_rmat(scale, ef):
     hg = HostGraph.rmat(scale, ef, seed=3)
