@@ -102,9 +102,14 @@ typedef struct mg_host_csr {
 } mg_host_csr;
 
 /* ---------------------------------------------------------------- library -- */
+/* Fills *opts with the defaults (what a NULL options pointer means). */
 void mg_options_init(mg_options *opts);
+/* Message of the most recent failure on this thread; the graph and algorithm
+ * calls clear it when they start. */
 const char *mg_last_error(void);
+/* Name of a status code (MG_OK, MG_ERR_ARG, ...). */
 const char *mg_status_string(int status);
+/* MG_ABI_VERSION of the built library; compare with the header's. */
 int mg_abi_version(void);
 /* Number of device-side kernel launches issued by this thread since the last reset. */
 int64_t mg_kernel_launches(int reset);
@@ -140,6 +145,7 @@ int mg_graph_create_batch(const int32_t *row_offsets, const int32_t *column_indi
                           int32_t ngraphs, const mg_options *opts, mg_graph **out);
 /* Free all device memory of the graph (GraphSlice::~GraphSlice, csr_problem.cuh:234-353). */
 int mg_graph_destroy(mg_graph *g);
+/* Vertex and edge counts, directedness and device bytes held by the graph. */
 int mg_graph_info(const mg_graph *g, int64_t *nodes, int64_t *edges, int32_t *directed,
                   int64_t *device_bytes);
 
@@ -264,12 +270,13 @@ int mg_build_weights(mg_host_csr *csr, uint32_t lo, uint32_t hi, uint64_t seed);
  * inserts the reverse of every edge, rows stably sorted by (row, col), self-loops
  * and duplicates kept. A "pattern" file gets value 1 on every edge. */
 int mg_read_market(const char *path, int32_t undirected, mg_host_csr *out);
-/* Transpose (CSC) of a host CSR: column offsets and row indices, stable by row. */
 /* CSV graph (GASengine/csv_graph_reader.cuh): format 0 = rows "src,dst:val,...",
  * format 1 = rows "src,dst,val"; ids renumbered densely in sorted order;
  * undirected != 0 adds the reversed edges. Edge values are int32. */
 int mg_read_csv(const char *path, int32_t format, int32_t undirected, mg_host_csr *out);
+/* Transpose (CSC) of a host CSR: column offsets and row indices, stable by row. */
 int mg_host_csr_transpose(const mg_host_csr *in, mg_host_csr *out);
+/* Frees the arrays of a host CSR filled by the builders and readers above. */
 void mg_host_csr_free(mg_host_csr *csr);
 
 #ifdef __cplusplus
