@@ -467,8 +467,8 @@ MG_DEVINL u64 warp_or(u64 x) {
 }
 
 // in-edges each pulling list probes lane by lane before the warp sweeps it
-// (probing lists of up to 4, 6 or 8 in-edges whole instead was 0-10 us slower
-// per run at R-MAT 22)
+// (probing lists of up to 4, 6 or 8 in-edges whole instead was no faster per run
+// at R-MAT 22: 5 to 11 us slower on one machine, within 5 us on another)
 constexpr int kMsProbe = 2;
 constexpr int kMsHeavyK = 4;  // loads per lane and round of a long in-list
 constexpr int kMsSub = 4;     // 32-edge sub-chunks whose loads are in flight together
@@ -973,8 +973,9 @@ __global__ void __launch_bounds__(256) k_ms_transpose_stk(const u64 *stk, const 
   uint8_t *tb = reinterpret_cast<uint8_t *>(tile[warp]);
   // The CTA takes 8 consecutive groups at a time and its warps start each step
   // together, so the grid's stores move through every source row as one narrow
-  // front (with the warps on their own, about 6 us slower per run at R-MAT 22;
-  // four consecutive groups per warp, a wider front, 35 us slower).
+  // front (with the warps on their own, 6 to 11 us slower per run at R-MAT 22
+  // and 17 us slower in a cold capture; four consecutive groups per warp, a
+  // wider front, 35 us slower).
   for (uint32_t base = blockIdx.x * kNW; base < groups; base += gridDim.x * kNW) {
     __syncthreads();  // every warp of the CTA runs the same steps
     const uint32_t grp = base + warp;
