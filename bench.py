@@ -628,6 +628,8 @@ def main():
 
         import torch
 
+        # each rank on its own GPU before NCCL sets up its communicator
+        torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
         torch.distributed.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
     try:
         res, hg, srcs = run_native(args, world)
